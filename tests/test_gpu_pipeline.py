@@ -1,0 +1,138 @@
+"""Whole-run parity of vb_pipeline (orbit -> stage 1 -> stage 2, one CUDA
+graph) against the FP64 CPU oracle on the pipeline's own inputs, plus graph
+vs eager, run-to-run determinism and the host-buffer entry point.
+
+Upstream orchestration: main_recon_online.cu:150-512,
+main_recon_online_mirror_tile_vissfast.cu:151-604.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from conftest import rel_err
+from gpu_util import tile_classes
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-5
+
+
+def host_inputs(p):
+    keys = ("u", "v", "w", "x1", "y1", "z1", "x2", "y2", "z2", "invn1", "invn2", "cosphi1", "cosphi2")
+    bl = {k: p.get(k) for k in keys}
+    bl = {k: v for k, v in bl.items() if v.size}
+    bl["nbl"] = p.nbl
+    bl["cosphi"] = p.cosphi
+    sky = {k: p.get(k) for k in ("B", "l", "m", "n")}
+    return sky, bl
+
+
+def pipeline_tile_classes(vb, p):
+    sky = vb.Sky()
+    sky.npix = p.npix
+    for k in ("B", "l", "m", "n", "cx", "cy", "cz", "cosA", "sinA"):
+        setattr(sky, k, p.ptr(k)[0])
+    sky.tile_pix = p.cfg.viss_tile_pix
+    bl = vb.Baselines()
+    bl.n_full, bl.nbl, bl.cosphi = 2 * p.n_half, p.nbl, p.cosphi
+    for k in ("u", "v", "w", "x1", "y1", "z1", "x2", "y2", "z2", "invn1", "invn2"):
+        setattr(bl, k, p.ptr(k)[0])
+    cls, tile = tile_classes(sky, bl, cull=vb.CULL_TILECONE)
+    return cls, tile
+
+
+@pytest.mark.parametrize("model", ["synthetic", "reference"])
+def test_pipeline_vs_oracle(gpu, vb, orc, model):
+    if model == "synthetic":
+        cfg = vb.run_config(nside=16, orbit_model=vb.ORBIT_SYNTHETIC, nsat=8, tsteps=64, segs=4, lambda_m=30.0,
+                            occ_R_m=6371e3, cull="tilecone", viss_tile_pix=256, mirror=1, grid_res=129,
+                            bl_max_m=100e3)
+    else:
+        cfg = vb.run_config(nside=8, orbit_model=vb.ORBIT_REFERENCE, segs=4, lambda_m=vb.btag_lambda("1M"),
+                            cull="tilecone", viss_tile_pix=256, mirror=1)
+    with vb.Pipeline(cfg) as p:
+        B = vb.synthetic_sky(16 if model == "synthetic" else 8, seed=2)
+        p.set_sky(B)
+        p.make_baselines()
+        rep = p.run()
+        assert rep["error_flags"] == 0
+        Vh = p.get("V_half")
+        Cd = p.get("C")
+        Wd = p.get("W")
+        sky, bl = host_inputs(p)
+        cls, tile = pipeline_tile_classes(vb, p)
+        Vo = orc.stage1(sky, bl, phase_corrected=1, tile_pix=tile, tile_cls=cls, precision=1)
+        emax, erms = rel_err(Vh, Vo)
+        assert emax <= TOL and erms <= TOL, (emax, erms)
+        t0, tl = p.seg_plan()
+        sp = p.seg_params()
+        Co, Wo, osp = orc.stage2(sky, bl, Vh, t0, tl, mirror=1, blockage=1, occ_mode=2, bl_max=cfg.bl_max_m,
+                                 lam=cfg.lambda_m, grid_res=cfg.grid_res, precision=1)
+        assert [s["nuniq"] for s in sp] == list(osp["nuniq"])
+        assert [np.float32(s["fa"]) for s in sp] == list(osp["fa"])
+        assert np.array_equal(Wd, Wo)
+        emax, erms = rel_err(Cd, Co)
+        assert emax <= TOL and erms <= TOL, (emax, erms)
+        assert rep["stage1_terms"] == p.npix * p.n_half
+        assert rep["stage2_terms"] == p.npix * sum(s["nuniq"] for s in sp)
+
+
+def test_graph_eager_determinism_and_host_entry(gpu, vb):
+    kw = dict(nside=16, orbit_model=vb.ORBIT_SYNTHETIC, nsat=8, tsteps=48, segs=3, lambda_m=30.0, occ_R_m=6371e3,
+              cull="exact", mirror=1, grid_res=101)
+    B = vb.synthetic_sky(16, seed=9)
+    outs = []
+    for use_graph in (1, 0, 1):
+        with vb.Pipeline(vb.run_config(use_graph=use_graph, **kw)) as p:
+            p.set_sky(B)
+            p.make_baselines()
+            p.run()
+            p.run()
+            outs.append((p.get("C"), p.get("V_half"), p.get("W")))
+            Ch, Vh, r = p.run_host(B, want_v=True)
+            assert np.array_equal(Ch.view(np.uint32), outs[-1][0].view(np.uint32))
+            assert np.array_equal(Vh.view(np.uint32), outs[-1][1].view(np.uint32))
+    for o in outs[1:]:
+        for a, b in zip(o, outs[0]):
+            assert np.array_equal(np.asarray(a).view(np.uint32), np.asarray(b).view(np.uint32))
+
+
+def test_precision_modes_against_fp64_pipeline(gpu, vb):
+    """The mixed-precision builds against the plain FP64 build of the same
+    pipeline (same tile classes, groups): <= 1e-5 normwise for V and C."""
+    kw = dict(nside=32, orbit_model=vb.ORBIT_SYNTHETIC, nsat=8, tsteps=128, segs=4, lambda_m=30.0,
+              occ_R_m=6371e3, cull="tilecone", viss_tile_pix=1024, mirror=1, grid_res=257)
+    B = vb.synthetic_sky(32, seed=4)
+    res = {}
+    for prec in ("fp64", "fp32_fp64phase", "fp32_dsphase", "ref32"):
+        with vb.Pipeline(vb.run_config(precision=prec, **kw)) as p:
+            p.set_sky(B)
+            p.make_baselines()
+            p.run()
+            res[prec] = (p.get("V_half"), p.get("C"))
+    for prec in ("fp32_fp64phase", "fp32_dsphase"):
+        for i in (0, 1):
+            emax, erms = rel_err(res[prec][i], res["fp64"][i])
+            assert emax <= TOL and erms <= TOL, (prec, i, emax, erms)
+    # the upstream FP32 arithmetic is measurably worse (documents why the phase needs FP64)
+    assert rel_err(res["ref32"][0], res["fp64"][0])[1] > 1e-5
+
+
+def test_halfsym_violation_is_reported(gpu, vb):
+    with vb.Pipeline(vb.run_config(nside=8, orbit_model=vb.ORBIT_SYNTHETIC, nsat=4, tsteps=8, segs=2,
+                                   lambda_m=30.0, occ_R_m=6371e3, grid_res=33)) as p:
+        p.set_sky(vb.synthetic_sky(8))
+        p.make_baselines()
+        ptr, n = p.ptr("u")
+        uh = np.empty(n, np.float32)
+        vb.check(vb.lib().vb_memcpy(uh.ctypes.data, ptr, uh.nbytes, 1))
+        uh[5] += 3.0
+        vb.check(vb.lib().vb_memcpy(ptr, uh.ctypes.data, uh.nbytes, 0))
+        bad = C.c_int()
+        vp_, _ = p.ptr("v")
+        wp_, _ = p.ptr("w")
+        rc = vb.lib().vb_validate_uvw_halfsym(ptr, vp_, wp_, n, p.nbl, C.byref(bad), None)
+        assert rc == 6 and bad.value == 5

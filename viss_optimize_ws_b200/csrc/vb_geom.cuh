@@ -1,0 +1,87 @@
+// Device functions whose float results decide discrete outcomes (occlusion
+// masks, tile classes, uv-cell keys).  They are written as the same float
+// expressions as the upstream kernels and every translation unit of this
+// library is compiled with the upstream flags (-O3 --use_fast_math, FMA
+// contraction on), so the compiler lowers them to the same instructions and
+// the decisions are bit-identical.  Parity tests pin this against the
+// upstream kernels themselves.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "vb_internal.h"
+
+namespace vb {
+
+// Per-pixel occlusion dot of one endpoint: (l x + m y + n z) * invn.
+// Upstream: viss_recon_kernel.cuh:271-272 (stage 1),
+// viss_recon_kernel_mirror_tile_vissfast.cuh:1101-1102 (stage 2).
+__device__ __forceinline__ float occ_dot(float lp, float mp, float np, float x, float y,
+                                         float z, float invn) {
+  return (lp * x + mp * y + np * z) * invn;
+}
+
+// Tile-cone three-way test of one endpoint direction against a tile cone
+// (centre dot `dotc`, cone cosA/sinA), upstream
+// viss_recon_kernel_mirror_tile_vissfast.cuh:91-98.
+__device__ __forceinline__ void cone_classify(float dotc, float cosA, float sinA, float cosphi,
+                                              bool& all_vis, bool& all_hid) {
+  dotc = fminf(1.0f, fmaxf(-1.0f, dotc));
+  float sind = sqrtf(fmaxf(0.0f, 1.0f - dotc * dotc));
+  float lower = dotc * cosA - sind * sinA;
+  float upper = dotc * cosA + sind * sinA;
+  all_vis = (lower >= cosphi);
+  all_hid = (upper < cosphi);
+}
+
+// Unit endpoint direction used by the tile test: (x, y, z) * invn, then the
+// dot with the tile centre, upstream ..._vissfast.cuh:484-485, 525-526.
+__device__ __forceinline__ float cone_dot(float ux, float uy, float uz, float cx, float cy,
+                                          float cz) {
+  return ux * cx + uy * cy + uz * cz;
+}
+
+// Round half away from zero, upstream viss_recon_kernel.cuh:13.
+__device__ __forceinline__ int round_half_away(float x) {
+  return (x >= 0.0f) ? (int)floorf(x + 0.5f) : (int)ceilf(x - 0.5f);
+}
+
+// Full-grid key of one signed baseline, upstream viss_recon_kernel.cuh:303-311.
+__device__ __forceinline__ int uv_key_full(float uu, float vv, float inv_du, int RES, int half) {
+  int ui = round_half_away(uu * inv_du);
+  int vi = round_half_away(vv * inv_du);
+  int U = ui + half;
+  int V = vi + half;
+  if ((unsigned)U >= (unsigned)RES || (unsigned)V >= (unsigned)RES) return 0;
+  return U * RES + V + 1;
+}
+
+// Half-grid key of one positive half-baseline, upstream
+// viss_recon_kernel_mirror_tile_vissfast.cuh:742-748.
+__device__ __forceinline__ int uv_key_half(float uu, float vv, float inv_du, int RES, int half) {
+  int U = (int)floorf(uu * inv_du + 0.5f) + half;
+  int V = (int)floorf(vv * inv_du + 0.5f) + half;
+  if (U < 0 || U >= RES || V < 0 || V >= RES) return 0;
+  return U * RES + V + 1;
+}
+
+// Exact (margin-protected) classification of one endpoint against a cone:
+// 1 = every pixel of the tile passes the FP32 test, -1 = every pixel fails,
+// 0 = undecided.  The FP32 evaluation error of the test is < 2e-6 for unit
+// vectors; the margin is 1e-5.
+__device__ __forceinline__ int exact_class(const ExactCone& c, float x, float y, float z, float invn,
+                                           float cosphi) {
+  double rx = (double)x * invn, ry = (double)y * invn, rz = (double)z * invn;
+  double rn = sqrt(rx * rx + ry * ry + rz * rz);
+  double cd = (c.cx * rx + c.cy * ry + c.cz * rz) / rn;
+  cd = fmin(1.0, fmax(-1.0, cd));
+  double d = acos(cd);
+  double lo = (d + c.alpha >= 3.141592653589793) ? -1.0 : cos(d + c.alpha);
+  double hi = (d <= c.alpha) ? 1.0 : cos(d - c.alpha);
+  // scale by the endpoint norm (|r invn| = 1 +- 3e-7) conservatively
+  const double margin = 1e-5;
+  if (lo * rn - margin >= (double)cosphi && lo - margin >= (double)cosphi) return 1;
+  if (hi * rn + margin < (double)cosphi && hi + margin < (double)cosphi) return -1;
+  return 0;
+}
+
+}  // namespace vb

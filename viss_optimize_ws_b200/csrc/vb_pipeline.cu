@@ -1,0 +1,771 @@
+// Run context of one main_recon_online run on one GPU: every device buffer
+// is allocated once at create time; a run is orbit/baselines -> stage 1 ->
+// stage 2 on one stream, optionally replayed from a CUDA graph.
+// Upstream orchestration: main_recon_online.cu:5-586 and
+// main_recon_online_mirror_tile_vissfast.cu:6-709.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <random>
+#include <string>
+#include <vector>
+
+#include "vb_common.cuh"
+#include "vb_internal.h"
+
+// ---------------------------------------------------------------------------
+// errors
+// ---------------------------------------------------------------------------
+namespace vb {
+static thread_local char g_msg[1024] = "";
+
+int fail(int code, const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_msg, sizeof(g_msg), fmt, ap);
+  va_end(ap);
+  return code;
+}
+
+int cuda_fail(cudaError_t e, const char* what, const char* file, int line) {
+  const char* base = strrchr(file, '/');
+  snprintf(g_msg, sizeof(g_msg), "CUDA error %s (%s) in %s at %s:%d", cudaGetErrorName(e), cudaGetErrorString(e),
+           what, base ? base + 1 : file, line);
+  return VB_ERR_CUDA;
+}
+
+int sm_count() {
+  static thread_local int dev_cached = -1, sms = 0;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 148;
+  if (dev != dev_cached) {
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 148;
+    dev_cached = dev;
+  }
+  return sms;
+}
+}  // namespace vb
+
+using namespace vb;
+
+extern "C" int vb_version(void) { return 10000; }
+
+extern "C" const char* vb_error_string(int code) {
+  switch (code) {
+    case VB_OK: return "ok";
+    case VB_ERR_INVALID: return "invalid argument";
+    case VB_ERR_CUDA: return "CUDA error";
+    case VB_ERR_TIMEOUT: return "device wait timed out";
+    case VB_ERR_NOMEM: return "out of memory / workspace too small";
+    case VB_ERR_UNSUPPORTED: return "unsupported";
+    case VB_ERR_HALFSYM: return "uvw half-symmetry check failed";
+    case VB_ERR_IO: return "I/O error";
+    default: return "unknown error";
+  }
+}
+
+extern "C" const char* vb_last_error(void) { return g_msg; }
+
+extern "C" int vb_device_info(int* sm, int* cc_major, int* cc_minor) {
+  int dev = 0;
+  VB_CUDA(cudaGetDevice(&dev));
+  if (sm) VB_CUDA(cudaDeviceGetAttribute(sm, cudaDevAttrMultiProcessorCount, dev));
+  if (cc_major) VB_CUDA(cudaDeviceGetAttribute(cc_major, cudaDevAttrComputeCapabilityMajor, dev));
+  if (cc_minor) VB_CUDA(cudaDeviceGetAttribute(cc_minor, cudaDevAttrComputeCapabilityMinor, dev));
+  return VB_OK;
+}
+
+// ---------------------------------------------------------------------------
+// pipeline
+// ---------------------------------------------------------------------------
+struct vb_pipeline {
+  vb_run_config cfg{};
+  cudaStream_t s = nullptr;
+  int64_t npix = 0;
+  float cosphi = 0.f;
+  bool per_end_cosphi = false;
+  // sky
+  float *B = nullptr, *l = nullptr, *m = nullptr, *n = nullptr, *nm1 = nullptr;
+  int tile_pix = 0, ntile = 0;
+  float *cx = nullptr, *cy = nullptr, *cz = nullptr, *cosA = nullptr, *sinA = nullptr;
+  bool sky_set = false;
+  bool pixels_ready = false;
+  bool s2_cones_ready = false;
+  // baselines
+  vb_orbit* orb = nullptr;
+  int T = 0, nbl = 0, nseg = 0, n_full = 0, n_half = 0;
+  std::vector<int> h_t0, h_tlen;
+  int *d_t0 = nullptr, *d_tlen = nullptr;
+  float *u = nullptr, *v = nullptr, *w = nullptr, *x1 = nullptr, *y1 = nullptr, *z1 = nullptr;
+  float *x2 = nullptr, *y2 = nullptr, *z2 = nullptr, *in1 = nullptr, *in2 = nullptr, *cp1 = nullptr,
+        *cp2 = nullptr;
+  bool baselines_ready = false;
+  // stage 1
+  Stage1Plan p1{};
+  void* ws1 = nullptr;
+  size_t ws1_bytes = 0;
+  Stage1Buffers b1{};
+  double* Vd = nullptr;
+  float* Vh = nullptr;
+  float* Vf = nullptr;
+  // stage 2
+  Stage2Plan p2{};
+  void* ws2 = nullptr;
+  size_t ws2_bytes = 0;
+  float* C = nullptr;
+  uint32_t* W = nullptr;
+  vb_seg_params* segp = nullptr;
+  double* wsum = nullptr;
+  unsigned long long* counters = nullptr;  // [0..3] stage 1, [4..7] stage 2
+  // timing / graph
+  cudaEvent_t ev[6] = {};
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+  std::vector<void*> owned;
+};
+
+extern "C" void vb_run_config_defaults(vb_run_config* c) {
+  if (!c) return;
+  std::memset(c, 0, sizeof(*c));
+  c->nside = 64;
+  c->day = 1;
+  c->segs = 4;
+  c->blockage = 1;
+  c->occ_mode = 2;
+  c->orbit_seed = 42;
+  c->lambda_m = 30.0f;
+  c->viss_tile_pix = 256;
+  c->mirror = 1;
+  c->cull = VB_CULL_TILECONE;
+  c->precision = VB_PREC_FP32_FP64PH;
+  c->orbit_model = VB_ORBIT_REFERENCE;
+  c->nsat = 8;
+  c->tsteps = 0;
+  c->dt_s = 2.0;
+  c->alt_min_km = 400.0;
+  c->alt_max_km = 600.0;
+  c->spread_km = 50.0;
+  c->occ_R_m = 0.0;
+  c->bl_max_m = 100e3f;
+  c->grid_res = 0;
+  c->seg_plan = 0;
+  c->seg_min_half = 50;
+  c->seg_max_half = 2000;
+  c->seg_seed = 7;
+  c->stage2_cull = VB_CULL_EXACT;
+  c->use_graph = 1;
+  c->device = 0;
+}
+
+template <class T>
+static int dalloc(vb_pipeline* p, T** ptr, size_t count) {
+  *ptr = nullptr;
+  if (count == 0) count = 1;
+  cudaError_t e = cudaMalloc(reinterpret_cast<void**>(ptr), count * sizeof(T));
+  if (e != cudaSuccess)
+    return fail(VB_ERR_NOMEM, "cudaMalloc of %zu bytes failed: %s", count * sizeof(T), cudaGetErrorString(e));
+  p->owned.push_back(*ptr);
+  return VB_OK;
+}
+
+static void pipeline_free(vb_pipeline* p) {
+  if (!p) return;
+  if (p->gexec) cudaGraphExecDestroy(p->gexec);
+  if (p->graph) cudaGraphDestroy(p->graph);
+  for (auto& e : p->ev)
+    if (e) cudaEventDestroy(e);
+  if (p->orb) vb_orbit_destroy(p->orb);
+  for (void* q : p->owned) cudaFree(q);
+  if (p->s) cudaStreamDestroy(p->s);
+  delete p;
+}
+
+static vb_sky sky_of(const vb_pipeline* p) {
+  vb_sky k{};
+  k.npix = p->npix;
+  k.B = p->B; k.l = p->l; k.m = p->m; k.n = p->n;
+  k.tile_pix = p->tile_pix;
+  k.cx = p->cx; k.cy = p->cy; k.cz = p->cz; k.cosA = p->cosA; k.sinA = p->sinA;
+  return k;
+}
+
+static vb_baselines bl_of(const vb_pipeline* p) {
+  vb_baselines b{};
+  b.n_full = p->n_full;
+  b.nbl = p->nbl;
+  b.u = p->u; b.v = p->v; b.w = p->w;
+  b.x1 = p->x1; b.y1 = p->y1; b.z1 = p->z1; b.invn1 = p->in1;
+  b.x2 = p->x2; b.y2 = p->y2; b.z2 = p->z2; b.invn2 = p->in2;
+  b.cosphi1 = p->per_end_cosphi ? p->cp1 : nullptr;
+  b.cosphi2 = p->per_end_cosphi ? p->cp2 : nullptr;
+  b.cosphi = p->cosphi;
+  return b;
+}
+
+// Segment plan: even split of T (main_recon_online.cu:123-134) or seeded
+// uneven half-baseline counts rounded up to whole steps.
+static int make_seg_plan(const vb_run_config& c, int T_avail, int nbl, bool synthetic, std::vector<int>& t0,
+                         std::vector<int>& tlen) {
+  t0.clear();
+  tlen.clear();
+  if (c.seg_plan == 1) {
+    if (c.segs <= 0 || c.seg_min_half <= 0 || c.seg_max_half < c.seg_min_half)
+      return fail(VB_ERR_INVALID, "uneven plan: segs=%d range [%d,%d]", c.segs, c.seg_min_half, c.seg_max_half);
+    std::mt19937_64 rng(c.seg_seed);
+    int cur = 0;
+    for (int k = 0; k < c.segs; ++k) {
+      uint64_t span = (uint64_t)(c.seg_max_half - c.seg_min_half + 1);
+      int cnt = c.seg_min_half + (int)(rng() % span);
+      int steps = (cnt + nbl - 1) / nbl;
+      t0.push_back(cur);
+      tlen.push_back(steps);
+      cur += steps;
+    }
+    if (!synthetic && cur > T_avail)
+      return fail(VB_ERR_INVALID, "uneven plan needs %d steps but the orbit has %d", cur, T_avail);
+    return VB_OK;
+  }
+  int segs = c.segs;
+  if (segs <= 0) return fail(VB_ERR_INVALID, "segs=%d", segs);
+  if (segs > T_avail) segs = T_avail;
+  int base = T_avail / segs, rem = T_avail % segs, cur = 0;
+  for (int k = 0; k < segs; ++k) {
+    int len = base + (k < rem ? 1 : 0);
+    t0.push_back(cur);
+    tlen.push_back(len);
+    cur += len;
+  }
+  return VB_OK;
+}
+
+static int uneven_total_steps(const vb_run_config& c, int nbl) {
+  std::mt19937_64 rng(c.seg_seed);
+  int cur = 0;
+  for (int k = 0; k < c.segs; ++k) {
+    uint64_t span = (uint64_t)(c.seg_max_half - c.seg_min_half + 1);
+    int cnt = c.seg_min_half + (int)(rng() % span);
+    cur += (cnt + nbl - 1) / nbl;
+  }
+  return cur;
+}
+
+extern "C" int vb_pipeline_create(const vb_run_config* c, vb_pipeline** out) {
+  if (!c || !out) return fail(VB_ERR_INVALID, "vb_pipeline_create: null argument");
+  *out = nullptr;
+  if (c->nside <= 0 || (c->nside & (c->nside - 1)) || c->nside > 8192)
+    return fail(VB_ERR_INVALID, "nside=%d must be a power of two <= 8192", c->nside);
+  if (c->precision < VB_PREC_REF32 || c->precision > VB_PREC_FP32_DSPH)
+    return fail(VB_ERR_INVALID, "precision=%d", c->precision);
+  VB_CUDA(cudaSetDevice(c->device));
+  vb_pipeline* p = new vb_pipeline();
+  p->cfg = *c;
+  int rc = VB_OK;
+#define PTRY(x)                         \
+  do {                                  \
+    rc = (x);                           \
+    if (rc != VB_OK) {                  \
+      pipeline_free(p);                 \
+      return rc;                        \
+    }                                   \
+  } while (0)
+#define PCUDA(x)                                                       \
+  do {                                                                 \
+    cudaError_t e_ = (x);                                              \
+    if (e_ != cudaSuccess) {                                           \
+      rc = cuda_fail(e_, #x, __FILE__, __LINE__);                      \
+      pipeline_free(p);                                                \
+      return rc;                                                       \
+    }                                                                  \
+  } while (0)
+  PCUDA(cudaStreamCreateWithFlags(&p->s, cudaStreamNonBlocking));
+  for (auto& e : p->ev) PCUDA(cudaEventCreate(&e));
+
+  // physics: global horizon cosine of the upstream lunar set-up (main_recon_online.cu:83-86)
+  {
+    float R = 1737.1e3f, h = 300e3f;
+    float theta = asinf(R / (R + h));
+    float phi = (float)3.14159265358979323846 - theta;
+    p->cosphi = cosf(phi);
+  }
+  p->per_end_cosphi = c->occ_R_m > 0.0;
+
+  // sky geometry
+  const int nside = c->nside;
+  p->npix = 12LL * nside * nside;
+  PTRY(dalloc(p, &p->B, p->npix));
+  PTRY(dalloc(p, &p->l, p->npix));
+  PTRY(dalloc(p, &p->m, p->npix));
+  PTRY(dalloc(p, &p->n, p->npix));
+  PTRY(dalloc(p, &p->nm1, p->npix));
+  PCUDA(cudaMemsetAsync(p->B, 0, p->npix * sizeof(float), p->s));
+  PTRY(vb_pix2lmn_nest(nside, 0, p->npix, p->l, p->m, p->n, p->s));
+  PTRY(vb_build_nm1(p->n, p->nm1, p->npix, p->s));
+  if (c->cull == VB_CULL_TILECONE && c->blockage) {
+    p->tile_pix = c->viss_tile_pix > 0 ? c->viss_tile_pix : 256;
+    if (p->tile_pix & (p->tile_pix - 1)) PTRY(fail(VB_ERR_INVALID, "viss_tile_pix=%d must be a power of two", p->tile_pix));
+    p->ntile = (int)ceil_div(p->npix, p->tile_pix);
+    PTRY(dalloc(p, &p->cx, p->ntile));
+    PTRY(dalloc(p, &p->cy, p->ntile));
+    PTRY(dalloc(p, &p->cz, p->ntile));
+    PTRY(dalloc(p, &p->cosA, p->ntile));
+    PTRY(dalloc(p, &p->sinA, p->ntile));
+    PTRY(vb_tile_cone_meta(p->tile_pix, p->l, p->m, p->n, p->npix, p->cx, p->cy, p->cz, p->cosA, p->sinA, p->s));
+  }
+
+  // orbit generator
+  vb_orbit_params op{};
+  op.model = c->orbit_model;
+  op.lambda_m = c->lambda_m;
+  op.day = c->day;
+  op.seed = c->orbit_seed;
+  op.nsat = c->orbit_model == VB_ORBIT_REFERENCE ? 8 : c->nsat;
+  op.dt_s = c->dt_s;
+  op.alt_min_km = c->alt_min_km;
+  op.alt_max_km = c->alt_max_km;
+  op.spread_km = c->spread_km;
+  op.occ_R_m = c->occ_R_m;
+  if (c->orbit_model == VB_ORBIT_SYNTHETIC) {
+    int nbl = op.nsat * (op.nsat - 1) / 2;
+    op.tsteps = (c->seg_plan == 1) ? uneven_total_steps(*c, nbl) : c->tsteps;
+  }
+  PTRY(vb_orbit_create(&op, &p->orb));
+  PTRY(vb_orbit_info(p->orb, &p->T, &p->nbl, nullptr, nullptr, nullptr));
+  PTRY(make_seg_plan(*c, p->T, p->nbl, c->orbit_model == VB_ORBIT_SYNTHETIC, p->h_t0, p->h_tlen));
+  p->nseg = (int)p->h_t0.size();
+  int steps = 0;
+  for (int k = 0; k < p->nseg; ++k) steps += p->h_tlen[k];
+  int64_t nfull = (int64_t)2 * p->nbl * steps;
+  if (nfull > INT32_MAX / 2) PTRY(fail(VB_ERR_UNSUPPORTED, "too many baselines (%lld)", (long long)nfull));
+  p->n_full = (int)nfull;
+  p->n_half = p->n_full / 2;
+  PTRY(dalloc(p, &p->d_t0, p->nseg));
+  PTRY(dalloc(p, &p->d_tlen, p->nseg));
+  PCUDA(cudaMemcpy(p->d_t0, p->h_t0.data(), p->nseg * sizeof(int), cudaMemcpyHostToDevice));
+  PCUDA(cudaMemcpy(p->d_tlen, p->h_tlen.data(), p->nseg * sizeof(int), cudaMemcpyHostToDevice));
+  float** arrs[] = {&p->u, &p->v, &p->w, &p->x1, &p->y1, &p->z1, &p->x2, &p->y2, &p->z2, &p->in1, &p->in2};
+  for (float** a : arrs) PTRY(dalloc(p, a, p->n_full));
+  if (p->per_end_cosphi) {
+    PTRY(dalloc(p, &p->cp1, p->n_full));
+    PTRY(dalloc(p, &p->cp2, p->n_full));
+  }
+
+  // stage 1 plan + workspace
+  vb_sky sky = sky_of(p);
+  vb_baselines bl = bl_of(p);
+  vb_stage1_opts o1{};
+  o1.precision = c->precision;
+  o1.cull = c->cull;
+  o1.phase_corrected = 1;
+  o1.blockage = c->blockage;
+  PTRY(stage1_plan(&sky, &bl, &o1, &p->p1));
+  p->ws1_bytes = stage1_carve(p->p1, nullptr, 0, nullptr, true);
+  PTRY(dalloc(p, reinterpret_cast<char**>(&p->ws1), p->ws1_bytes));
+  stage1_carve(p->p1, p->ws1, p->ws1_bytes, &p->b1, true);
+  PTRY(dalloc(p, &p->Vd, (size_t)2 * p->n_half));
+  PTRY(dalloc(p, &p->Vh, (size_t)2 * p->n_half));
+  PTRY(dalloc(p, &p->Vf, (size_t)2 * p->n_full));
+
+  // stage 2 plan + workspace
+  vb_stage2_opts o2{};
+  o2.mirror = c->mirror;
+  o2.blockage = c->blockage;
+  o2.occ_mode = c->occ_mode;
+  o2.precision = c->precision;
+  o2.cull = c->stage2_cull;
+  o2.grid_res = c->grid_res;
+  o2.bl_max = c->bl_max_m;
+  o2.lambda = c->lambda_m;
+  PTRY(stage2_plan(p->n_half, p->nseg, p->npix, &o2, &p->p2));
+  p->ws2_bytes = stage2_workspace(p->p2, nullptr, 0, nullptr);
+  PTRY(dalloc(p, reinterpret_cast<char**>(&p->ws2), p->ws2_bytes));
+  PTRY(dalloc(p, &p->C, p->npix));
+  PTRY(dalloc(p, &p->W, p->npix));
+  PTRY(dalloc(p, &p->segp, p->nseg));
+  PTRY(dalloc(p, &p->wsum, 2));
+  PTRY(dalloc(p, &p->counters, 8));
+  PCUDA(cudaMemsetAsync(p->counters, 0, 8 * sizeof(unsigned long long), p->s));
+  PCUDA(cudaStreamSynchronize(p->s));
+#undef PTRY
+#undef PCUDA
+  *out = p;
+  return VB_OK;
+}
+
+__global__ void k_scale_sky(float* B, int64_t n, double scale) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    B[i] = (float)((double)B[i] * scale);
+}
+
+static int set_sky_async(vb_pipeline* p, const float* B_host, int scale) {
+  if (!B_host) return fail(VB_ERR_INVALID, "set_sky: null B");
+  VB_CUDA(cudaMemcpyAsync(p->B, B_host, p->npix * sizeof(float), cudaMemcpyHostToDevice, p->s));
+  if (scale) {
+    // B *= 4 pi / npix in FP64 (main_recon_online.cu:106-112)
+    const double pix_area = 4.0 * 3.14159265358979323846 / (double)p->npix;
+    int g = (int)std::min<int64_t>(ceil_div(p->npix, 256), (int64_t)sm_count() * 16);
+    k_scale_sky<<<g, 256, 0, p->s>>>(p->B, p->npix, pix_area);
+    VB_LAUNCH_CHECK();
+  }
+  p->sky_set = true;
+  p->pixels_ready = false;
+  return VB_OK;
+}
+
+extern "C" int vb_pipeline_set_sky(vb_pipeline* p, const float* B_host, int scale) {
+  if (!p) return fail(VB_ERR_INVALID, "vb_pipeline_set_sky: null pipeline");
+  VB_TRY(set_sky_async(p, B_host, scale));
+  VB_CUDA(cudaStreamSynchronize(p->s));
+  return VB_OK;
+}
+
+static int make_baselines_async(vb_pipeline* p) {
+  VB_TRY(vb_orbit_make_segment(p->orb, 0, p->n_full / (2 * p->nbl), p->u, p->v, p->w, p->x1, p->y1, p->z1, p->x2,
+                               p->y2, p->z2, p->per_end_cosphi ? p->cp1 : nullptr,
+                               p->per_end_cosphi ? p->cp2 : nullptr, p->s));
+  VB_TRY(geom_invnorm(p->x1, p->y1, p->z1, p->in1, p->n_full, p->s));
+  VB_TRY(geom_invnorm(p->x2, p->y2, p->z2, p->in2, p->n_full, p->s));
+  return VB_OK;
+}
+
+extern "C" int vb_pipeline_make_baselines(vb_pipeline* p) {
+  if (!p) return fail(VB_ERR_INVALID, "vb_pipeline_make_baselines: null pipeline");
+  VB_TRY(make_baselines_async(p));
+  int bad = -1;
+  VB_TRY(vb_validate_uvw_halfsym(p->u, p->v, p->w, p->n_full, p->nbl, &bad, p->s));
+  p->baselines_ready = true;
+  return VB_OK;
+}
+
+// Both stages on p->s (capturable).
+static int enqueue_stages(vb_pipeline* p) {
+  vb_sky sky = sky_of(p);
+  vb_baselines bl = bl_of(p);
+  VB_CUDA(cudaMemsetAsync(p->counters, 0, 8 * sizeof(unsigned long long), p->s));
+  VB_CUDA(cudaEventRecord(p->ev[0], p->s));
+  VB_TRY(stage1_run(&sky, &bl, p->p1, p->b1, true, p->Vd, p->counters, p->s));
+  VB_TRY(phase_correct_expand_async(p->Vd, p->w, p->n_half, p->nbl, 1, p->Vh, p->Vf, p->s));
+  VB_CUDA(cudaEventRecord(p->ev[1], p->s));
+  Stage2Pixels pre;
+  pre.lm = p->b1.lm;
+  pre.nb = p->b1.nb;
+  pre.f4 = p->b1.f4;
+  pre.cones_ready = p->s2_cones_ready;
+  VB_TRY(stage2_run(&sky, &bl, p->Vh, p->nseg, p->d_t0, p->d_tlen, p->p2, p->ws2, p->ws2_bytes, p->C, p->W,
+                    p->segp, p->counters + 4, p->wsum, p->s, &pre));
+  VB_CUDA(cudaEventRecord(p->ev[2], p->s));
+  return VB_OK;
+}
+
+static int fill_report(vb_pipeline* p, vb_report* r) {
+  if (!r) return VB_OK;
+  std::memset(r, 0, sizeof(*r));
+  r->npix_hi = (int)(p->npix >> 31);
+  r->npix_lo = (int)(p->npix & 0x7fffffff);
+  r->nseg = p->nseg;
+  r->n_half_total = p->n_half;
+  float t1 = 0.f, t2 = 0.f;
+  VB_CUDA(cudaEventElapsedTime(&t1, p->ev[0], p->ev[1]));
+  VB_CUDA(cudaEventElapsedTime(&t2, p->ev[1], p->ev[2]));
+  r->t_stage1_ms = t1;
+  r->t_stage2_ms = t2;
+  unsigned long long cnt[8];
+  VB_CUDA(cudaMemcpy(cnt, p->counters, sizeof(cnt), cudaMemcpyDeviceToHost));
+  for (int k = 0; k < 4; ++k) {
+    r->s1_counters[k] = cnt[k];
+    r->s2_counters[k] = cnt[4 + k];
+  }
+  std::vector<vb_seg_params> sp(p->nseg);
+  VB_CUDA(cudaMemcpy(sp.data(), p->segp, p->nseg * sizeof(vb_seg_params), cudaMemcpyDeviceToHost));
+  double ws = 0;
+  VB_CUDA(cudaMemcpy(&ws, p->wsum, sizeof(double), cudaMemcpyDeviceToHost));
+  r->w_scalar_total = ws;
+  long long g = 0;
+  for (auto& q : sp) g += q.nuniq;
+  r->groups_total = g;
+  r->stage1_terms = (long long)p->npix * p->n_half;
+  r->stage2_terms = (long long)p->npix * g;
+  unsigned e1 = 0;
+  VB_CUDA(cudaMemcpy(&e1, p->b1.err, sizeof(unsigned), cudaMemcpyDeviceToHost));
+  r->error_flags = (int)e1;
+  return VB_OK;
+}
+
+static int ensure_ready(vb_pipeline* p) {
+  if (!p->sky_set) return fail(VB_ERR_INVALID, "pipeline: sky not set");
+  if (!p->baselines_ready) VB_TRY(vb_pipeline_make_baselines(p));
+  if (!p->pixels_ready) {
+    vb_sky sky = sky_of(p);
+    VB_TRY(stage1_prepare_pixels(&sky, p->p1, p->b1, p->s));
+    VB_CUDA(cudaMemsetAsync(p->b1.err, 0, sizeof(unsigned), p->s));
+    p->pixels_ready = true;
+    if (p->gexec) {   // pixel records are rebuilt in place: the graph stays valid
+    }
+  }
+  return VB_OK;
+}
+
+static int run_once(vb_pipeline* p) {
+  if (p->cfg.use_graph) {
+    if (!p->gexec) {
+      // eager run first (sets kernel attributes, computes stage-2 block cones)
+      VB_TRY(enqueue_stages(p));
+      VB_CUDA(cudaStreamSynchronize(p->s));
+      p->s2_cones_ready = true;
+      VB_CUDA(cudaStreamBeginCapture(p->s, cudaStreamCaptureModeThreadLocal));
+      int rc = enqueue_stages(p);
+      cudaGraph_t g = nullptr;
+      cudaError_t e = cudaStreamEndCapture(p->s, &g);
+      if (rc != VB_OK) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+      }
+      if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture", __FILE__, __LINE__);
+      p->graph = g;
+      VB_CUDA(cudaGraphInstantiate(&p->gexec, g, 0));
+    }
+    VB_CUDA(cudaGraphLaunch(p->gexec, p->s));
+  } else {
+    VB_TRY(enqueue_stages(p));
+    p->s2_cones_ready = true;
+  }
+  return VB_OK;
+}
+
+extern "C" int vb_pipeline_run(vb_pipeline* p, vb_report* r) {
+  if (!p) return fail(VB_ERR_INVALID, "vb_pipeline_run: null pipeline");
+  VB_CUDA(cudaSetDevice(p->cfg.device));
+  VB_TRY(ensure_ready(p));
+  VB_TRY(run_once(p));
+  VB_CUDA(cudaStreamSynchronize(p->s));
+  VB_TRY(fill_report(p, r));
+  return VB_OK;
+}
+
+extern "C" int vb_pipeline_run_host(vb_pipeline* p, const float* B_host, int scale, float* C_host,
+                                    float* V_half_host, vb_report* r) {
+  if (!p || !C_host) return fail(VB_ERR_INVALID, "vb_pipeline_run_host: null argument");
+  VB_CUDA(cudaSetDevice(p->cfg.device));
+  VB_CUDA(cudaEventRecord(p->ev[3], p->s));
+  VB_TRY(set_sky_async(p, B_host, scale));
+  VB_TRY(make_baselines_async(p));
+  p->baselines_ready = true;
+  vb_sky sky = sky_of(p);
+  VB_TRY(stage1_prepare_pixels(&sky, p->p1, p->b1, p->s));
+  p->pixels_ready = true;
+  VB_TRY(run_once(p));
+  VB_CUDA(cudaMemcpyAsync(C_host, p->C, p->npix * sizeof(float), cudaMemcpyDeviceToHost, p->s));
+  if (V_half_host)
+    VB_CUDA(cudaMemcpyAsync(V_half_host, p->Vh, (size_t)2 * p->n_half * sizeof(float), cudaMemcpyDeviceToHost, p->s));
+  VB_CUDA(cudaEventRecord(p->ev[4], p->s));
+  VB_CUDA(cudaStreamSynchronize(p->s));
+  VB_TRY(fill_report(p, r));
+  if (r) {
+    float te = 0.f;
+    VB_CUDA(cudaEventElapsedTime(&te, p->ev[3], p->ev[4]));
+    r->t_orbit_ms = te;   // whole end-to-end call (H2D, baselines, both stages, D2H)
+  }
+  return VB_OK;
+}
+
+extern "C" int vb_pipeline_device_ptr(vb_pipeline* p, const char* name, void** ptr, int64_t* count) {
+  if (!p || !name || !ptr) return fail(VB_ERR_INVALID, "vb_pipeline_device_ptr: null argument");
+  struct E { const char* k; void* v; int64_t n; };
+  const E tab[] = {
+      {"C", p->C, p->npix}, {"W", p->W, p->npix}, {"V_half", p->Vh, 2LL * p->n_half},
+      {"V_full", p->Vf, 2LL * p->n_full}, {"V_half_d", p->Vd, 2LL * p->n_half},
+      {"u", p->u, p->n_full}, {"v", p->v, p->n_full}, {"w", p->w, p->n_full},
+      {"x1", p->x1, p->n_full}, {"y1", p->y1, p->n_full}, {"z1", p->z1, p->n_full},
+      {"x2", p->x2, p->n_full}, {"y2", p->y2, p->n_full}, {"z2", p->z2, p->n_full},
+      {"invn1", p->in1, p->n_full}, {"invn2", p->in2, p->n_full},
+      {"cosphi1", p->cp1, p->cp1 ? p->n_full : 0}, {"cosphi2", p->cp2, p->cp2 ? p->n_full : 0},
+      {"l", p->l, p->npix}, {"m", p->m, p->npix}, {"n", p->n, p->npix}, {"B", p->B, p->npix},
+      {"nm1", p->nm1, p->npix}, {"cx", p->cx, p->ntile}, {"cy", p->cy, p->ntile}, {"cz", p->cz, p->ntile},
+      {"cosA", p->cosA, p->ntile}, {"sinA", p->sinA, p->ntile}, {"seg_t0", p->d_t0, p->nseg},
+      {"seg_tlen", p->d_tlen, p->nseg}, {"seg_params", p->segp, p->nseg},
+  };
+  for (const E& e : tab)
+    if (std::strcmp(e.k, name) == 0) {
+      *ptr = e.v;
+      if (count) *count = e.n;
+      return VB_OK;
+    }
+  return fail(VB_ERR_INVALID, "vb_pipeline_device_ptr: unknown buffer '%s'", name);
+}
+
+extern "C" int vb_pipeline_info(vb_pipeline* p, int64_t* npix, int* nseg, int* n_half_total, int* nbl, int* ntile,
+                                float* cosphi) {
+  if (!p) return fail(VB_ERR_INVALID, "vb_pipeline_info: null pipeline");
+  if (npix) *npix = p->npix;
+  if (nseg) *nseg = p->nseg;
+  if (n_half_total) *n_half_total = p->n_half;
+  if (nbl) *nbl = p->nbl;
+  if (ntile) *ntile = p->ntile;
+  if (cosphi) *cosphi = p->cosphi;
+  return VB_OK;
+}
+
+extern "C" int vb_pipeline_seg_plan(vb_pipeline* p, int* t0, int* tlen) {
+  if (!p) return fail(VB_ERR_INVALID, "vb_pipeline_seg_plan: null pipeline");
+  for (int k = 0; k < p->nseg; ++k) {
+    if (t0) t0[k] = p->h_t0[k];
+    if (tlen) tlen[k] = p->h_tlen[k];
+  }
+  return VB_OK;
+}
+
+extern "C" int vb_pipeline_seg_params(vb_pipeline* p, vb_seg_params* out) {
+  if (!p || !out) return fail(VB_ERR_INVALID, "vb_pipeline_seg_params: null argument");
+  VB_CUDA(cudaStreamSynchronize(p->s));
+  VB_CUDA(cudaMemcpy(out, p->segp, p->nseg * sizeof(vb_seg_params), cudaMemcpyDeviceToHost));
+  return VB_OK;
+}
+
+extern "C" int vb_pipeline_destroy(vb_pipeline* p) {
+  if (p) {
+    cudaSetDevice(p->cfg.device);
+    if (p->s) cudaStreamSynchronize(p->s);
+    pipeline_free(p);
+  }
+  return VB_OK;
+}
+
+// ---------------------------------------------------------------------------
+// measurement helpers
+// ---------------------------------------------------------------------------
+__global__ void k_peak_sfu(float* out, int iters, float seed) {
+  float a0 = seed + threadIdx.x * 1e-3f, a1 = a0 + 0.1f, a2 = a0 + 0.2f, a3 = a0 + 0.3f;
+  float b0 = a0 + 0.4f, b1 = a0 + 0.5f, b2 = a0 + 0.6f, b3 = a0 + 0.7f;
+  for (int i = 0; i < iters; ++i) {
+    a0 = __sinf(a0) + 1.25f; a1 = __sinf(a1) + 1.25f; a2 = __sinf(a2) + 1.25f; a3 = __sinf(a3) + 1.25f;
+    b0 = __cosf(b0) + 0.75f; b1 = __cosf(b1) + 0.75f; b2 = __cosf(b2) + 0.75f; b3 = __cosf(b3) + 0.75f;
+  }
+  float r = a0 + a1 + a2 + a3 + b0 + b1 + b2 + b3;
+  if (r == 12345.678f) out[0] = r;
+}
+
+__global__ void k_peak_fp32(float* out, int iters, float seed) {
+  float x[8];
+  for (int k = 0; k < 8; ++k) x[k] = seed + k + threadIdx.x * 1e-3f;
+  for (int i = 0; i < iters; ++i)
+#pragma unroll
+    for (int k = 0; k < 8; ++k) x[k] = fmaf(x[k], 0.999f, 0.001f);
+  float r = 0;
+  for (int k = 0; k < 8; ++k) r += x[k];
+  if (r == 12345.678f) out[0] = r;
+}
+
+__global__ void k_peak_fp64(double* out, int iters, double seed) {
+  double x[8];
+  for (int k = 0; k < 8; ++k) x[k] = seed + k + threadIdx.x * 1e-3;
+  for (int i = 0; i < iters; ++i)
+#pragma unroll
+    for (int k = 0; k < 8; ++k) x[k] = fma(x[k], 0.999, 0.001);
+  double r = 0;
+  for (int k = 0; k < 8; ++k) r += x[k];
+  if (r == 12345.678) out[0] = r;
+}
+
+__global__ void k_clock(long long* out, int iters) {
+  long long t0 = clock64();
+  float x = threadIdx.x;
+  for (int i = 0; i < iters; ++i) x = fmaf(x, 0.999f, 0.001f);
+  long long t1 = clock64();
+  if (threadIdx.x == 0 && blockIdx.x == 0) out[0] = t1 - t0;
+  if (x == 12345.678f) out[1] = 1;
+}
+
+extern "C" int vb_measure_peaks(double* sfu, double* fp32, double* fp64, double* clk_mhz) {
+  const int sms = sm_count();
+  const int blocks = sms * 8, threads = 256;
+  float* d = nullptr;
+  VB_CUDA(cudaMalloc(&d, 64));
+  cudaEvent_t a, b;
+  VB_CUDA(cudaEventCreate(&a));
+  VB_CUDA(cudaEventCreate(&b));
+  float ms = 0.f;
+  auto timeit = [&](auto launch) -> double {
+    launch();
+    cudaEventRecord(a);
+    launch();
+    cudaEventRecord(b);
+    cudaEventSynchronize(b);
+    cudaEventElapsedTime(&ms, a, b);
+    return ms * 1e-3;
+  };
+  const int it_sfu = 4096, it_f = 16384, it_d = 4096;
+  double t_sfu = timeit([&] { k_peak_sfu<<<blocks, threads>>>(d, it_sfu, 0.3f); });
+  double t_f = timeit([&] { k_peak_fp32<<<blocks, threads>>>(d, it_f, 0.3f); });
+  double t_d = timeit([&] { k_peak_fp64<<<blocks, threads>>>((double*)d, it_d, 0.3); });
+  // effective SM clock over a ~10 ms FP32 loop
+  long long* dc = reinterpret_cast<long long*>(d);
+  const int it_c = 2000000;
+  double t_c = timeit([&] { k_clock<<<sms, 32>>>(dc, it_c); });
+  long long cycles = 0;
+  VB_CUDA(cudaMemcpy(&cycles, dc, sizeof(long long), cudaMemcpyDeviceToHost));
+  cudaError_t e = cudaGetLastError();
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  cudaFree(d);
+  if (e != cudaSuccess) return cuda_fail(e, "peak kernels", __FILE__, __LINE__);
+  const double nthreads = (double)blocks * threads;
+  if (sfu) *sfu = nthreads * it_sfu * 8.0 / 2.0 / t_sfu;   // sin+cos pairs per second
+  if (fp32) *fp32 = nthreads * it_f * 8.0 / t_f;           // FMA per second
+  if (fp64) *fp64 = nthreads * it_d * 8.0 / t_d;           // DFMA per second
+  if (clk_mhz) *clk_mhz = (double)cycles / t_c / 1e6;
+  return VB_OK;
+}
+
+extern "C" int vb_flush_l2(void* buf, size_t bytes, void* stream) {
+  if (!buf || bytes == 0) return fail(VB_ERR_INVALID, "vb_flush_l2: empty buffer");
+  VB_CUDA(cudaMemsetAsync(buf, 0, bytes, as_stream(stream)));
+  return VB_OK;
+}
+
+// ---------------------------------------------------------------------------
+// host plumbing
+// ---------------------------------------------------------------------------
+extern "C" int vb_set_device(int device) {
+  VB_CUDA(cudaSetDevice(device));
+  return VB_OK;
+}
+extern "C" int vb_malloc(void** ptr, size_t bytes) {
+  if (!ptr) return fail(VB_ERR_INVALID, "vb_malloc: null ptr");
+  *ptr = nullptr;
+  cudaError_t e = cudaMalloc(ptr, bytes ? bytes : 1);
+  if (e != cudaSuccess) return fail(VB_ERR_NOMEM, "vb_malloc(%zu): %s", bytes, cudaGetErrorString(e));
+  return VB_OK;
+}
+extern "C" int vb_free(void* ptr) {
+  if (ptr) VB_CUDA(cudaFree(ptr));
+  return VB_OK;
+}
+extern "C" int vb_memcpy(void* dst, const void* src, size_t bytes, int kind) {
+  if (bytes == 0) return VB_OK;
+  if (!dst || !src) return fail(VB_ERR_INVALID, "vb_memcpy: null pointer");
+  cudaMemcpyKind k = kind == VB_H2D ? cudaMemcpyHostToDevice
+                   : kind == VB_D2H ? cudaMemcpyDeviceToHost
+                                    : cudaMemcpyDeviceToDevice;
+  VB_CUDA(cudaMemcpy(dst, src, bytes, k));
+  return VB_OK;
+}
+extern "C" int vb_memset(void* ptr, int value, size_t bytes) {
+  if (bytes == 0) return VB_OK;
+  VB_CUDA(cudaMemset(ptr, value, bytes));
+  return VB_OK;
+}
+extern "C" int vb_synchronize(void) {
+  VB_CUDA(cudaDeviceSynchronize());
+  return VB_OK;
+}
+extern "C" int vb_make_synthetic_sky(int nside, uint64_t seed, int n_points, float amp, float* B) {
+  if (nside <= 0 || !B || n_points < 0) return fail(VB_ERR_INVALID, "vb_make_synthetic_sky: bad args");
+  const int64_t npix = 12LL * nside * nside;
+  std::mt19937_64 rng(seed);
+  for (int64_t i = 0; i < npix; ++i) B[i] = (float)(rng() >> 40) * (1.0f / 16777216.0f);
+  for (int k = 0; k < n_points; ++k) {
+    int64_t idx = (int64_t)(rng() % (uint64_t)npix);
+    B[idx] += amp;
+  }
+  return VB_OK;
+}

@@ -1,0 +1,674 @@
+// Stage 1: half-conjugate visibility sum
+//   V[ih] = sum_p B_p * occ_a(p) * occ_b(p) * exp(-2 pi i t(ih, p)),
+//   t = u l + v m + w (n - 1)        (phase_corrected = 0, as the upstream kernel)
+//   t = u l + v m + w n              (phase_corrected = 1, = upstream V after
+//                                     phase_correct_viss_halfsym_host)
+// Upstream: viss_partial_all_halfsym<256,true> (viss_recon_kernel.cuh:200-287)
+// and viss_partial_all_halfsym_tilecone<TILE,true>
+// (viss_recon_kernel_mirror_tile_vissfast.cuh:437-561).
+//
+// B200 design: persistent CTAs pull (baseline tile x pixel chunk) items from a
+// device counter; each thread owns BPT half-baselines; pixels are staged in
+// shared memory as FP64 (l, m), (n, B) and FP32 (l, m, n, B) records and read
+// as warp-broadcasts.  Per pixel tile each warp takes one of three paths
+// (skip / unmasked / masked) from its lanes' tile classes, so the hot loop is
+// warp-uniform.  Partial sums per chunk are reduced in a fixed order
+// (deterministic).
+//
+// Precision modes (the `MODE` template argument):
+//   REF32  : FP32 phase (upstream arithmetic), FP32 sincos, FP32 stage sums.
+//   FP64   : FP64 phase, FP64 sincos, FP64 sums (the plain FP64 direct sum).
+//   F32X   : phase formed in FP64 with a magic-constant range reduction: the
+//            turn fraction lands in the low word of the double; its top 23
+//            bits become an exact FP32 angle in [0, 2pi); FP32 sincos; FP32
+//            sums per staged tile (<= 1024 terms), FP64 across tiles.
+//   DS     : each product split exactly (p = fl(a b), e = fma(a, b, -p)),
+//            fractions p - rint(p) exact in FP32; FP32 sincos; Kahan sums
+//            across tiles.
+#include <cmath>
+#include <algorithm>
+#include <type_traits>
+
+#include "vb_common.cuh"
+#include "vb_geom.cuh"
+#include "vb_internal.h"
+
+namespace vb {
+
+constexpr int S1_THREADS = 256;
+constexpr int kClsHid = 0, kClsVis = 1, kClsMix = 2;
+
+// F32X phase reduction: magic = 1.5 * 2^23 keeps every partial sum of the FMA
+// chain in [2^23, 2^24) while 4*max|uvw| < 2^22; the double's ulp is then
+// 2^-29 turns and bits [6, 29) of the low word are the top 23 fraction bits.
+constexpr double kMagic = 12582912.0;              // 1.5 * 2^23
+constexpr double kHalfLsb = 5.9604644775390625e-8; // 2^-24 turns: rounds the truncation
+constexpr int kFracShift = 6;
+constexpr float kTwoPiF = 6.28318530717958647692f;
+constexpr float kAngScale = 6.28318530717958647692f * 1.1920928955078125e-7f;  // fl(2pi) * 2^-23
+constexpr double kMaxUvwF32X = 1048576.0;          // 2^20
+
+struct S1Args {
+  const double2* __restrict__ lm;
+  const float4* __restrict__ nb;
+  const float4* __restrict__ f4;
+  int64_t npix;
+  int cull, cull_tile, stage_pix, chunk_pix, nchunk, n_btile, n_items;
+  const float *tcx, *tcy, *tcz, *tcosA, *tsinA;   // VB_CULL_TILECONE
+  const ExactCone* cones;                          // VB_CULL_EXACT
+  const float *u, *v, *w, *x1, *y1, *z1, *in1, *x2, *y2, *z2, *in2, *cp1, *cp2;
+  float cosphi;
+  int n_half, nbl, blockage, phase_corrected;
+  int* queue;
+  double2* partial;
+  unsigned long long* counters;
+  unsigned* err;
+};
+
+struct Baseline {
+  double U, V, W, C;
+  float uf, vf, wf, fw;   // FP32 copies; fw = -frac(w) (raw phase, DS)
+  float ku, kv, kw;       // REF32: -2 pi * (u, v, w)
+  float x1, y1, z1, i1, x2, y2, z2, i2, c1, c2;
+  float ux1, uy1, uz1, ux2, uy2, uz2;
+  int cls;
+  bool active;
+};
+
+__device__ __forceinline__ float rint_magic(float x) {
+  return __fsub_rn(__fadd_rn(x, 12582912.0f), 12582912.0f);
+}
+
+// Tile class of one baseline for one cull tile (0 hidden, 1 visible, 2 mixed).
+// Upstream decision: ..._vissfast.cuh:519-531 (tile cone), per-pixel mask
+// everywhere for the plain kernel (viss_recon_kernel.cuh:270-274).
+__device__ __forceinline__ int tile_class(const S1Args& a, const Baseline& b, int tile_id) {
+  if (!b.active) return kClsHid;
+  if (!a.blockage) return kClsVis;
+  if (a.cull == VB_CULL_TILECONE) {
+    const float cx = a.tcx[tile_id], cy = a.tcy[tile_id], cz = a.tcz[tile_id];
+    const float cA = a.tcosA[tile_id], sA = a.tsinA[tile_id];
+    bool vis1, hid1, vis2, hid2;
+    cone_classify(cone_dot(b.ux1, b.uy1, b.uz1, cx, cy, cz), cA, sA, b.c1, vis1, hid1);
+    cone_classify(cone_dot(b.ux2, b.uy2, b.uz2, cx, cy, cz), cA, sA, b.c2, vis2, hid2);
+    return (hid1 || hid2) ? kClsHid : ((vis1 && vis2) ? kClsVis : kClsMix);
+  }
+  if (a.cull == VB_CULL_EXACT) {
+    const ExactCone c = a.cones[tile_id];
+    int e1 = exact_class(c, b.x1, b.y1, b.z1, b.i1, b.c1);
+    int e2 = exact_class(c, b.x2, b.y2, b.z2, b.i2, b.c2);
+    return (e1 < 0 || e2 < 0) ? kClsHid : ((e1 > 0 && e2 > 0) ? kClsVis : kClsMix);
+  }
+  return kClsMix;
+}
+
+// Loads half-baseline ih into registers (upstream: viss_recon_kernel.cuh:231-240,
+// ..._vissfast.cuh:476-497).
+__device__ __forceinline__ void load_baseline(const S1Args& a, int ih, bool raw, Baseline& b) {
+  b.active = ih < a.n_half;
+  const int i = b.active ? half_to_full_pos(ih, a.nbl) : 0;
+  float uu = b.active ? a.u[i] : 0.f, vv = b.active ? a.v[i] : 0.f, ww = b.active ? a.w[i] : 0.f;
+  b.uf = uu; b.vf = vv; b.wf = ww;
+  b.U = uu; b.V = vv; b.W = ww;
+  b.C = kMagic + kHalfLsb - (raw ? (double)ww : 0.0);
+  b.fw = raw ? -__fsub_rn(ww, rint_magic(ww)) : 0.0f;
+  const float kk = -2.0f * 3.14159265358979323846f;
+  b.ku = kk * uu; b.kv = kk * vv; b.kw = kk * ww;
+  if (a.blockage && b.active) {
+    b.x1 = a.x1[i]; b.y1 = a.y1[i]; b.z1 = a.z1[i]; b.i1 = a.in1[i];
+    b.x2 = a.x2[i]; b.y2 = a.y2[i]; b.z2 = a.z2[i]; b.i2 = a.in2[i];
+    b.c1 = a.cp1 ? a.cp1[i] : a.cosphi;
+    b.c2 = a.cp2 ? a.cp2[i] : a.cosphi;
+  } else {
+    b.x1 = b.y1 = b.z1 = b.i1 = b.x2 = b.y2 = b.z2 = b.i2 = 0.f;
+    b.c1 = b.c2 = a.cosphi;
+  }
+  b.ux1 = b.x1 * b.i1; b.uy1 = b.y1 * b.i1; b.uz1 = b.z1 * b.i1;
+  b.ux2 = b.x2 * b.i2; b.uy2 = b.y2 * b.i2; b.uz2 = b.z2 * b.i2;
+  b.cls = kClsHid;
+}
+
+template <int MODE>
+__device__ __forceinline__ void phase_sincos(const Baseline& b, const double2 lm, const double nd,
+                                             const float4 f, const float nm1, float& s, float& c,
+                                             double& sd, double& cd, bool raw) {
+  if constexpr (MODE == VB_PREC_FP32_FP64PH) {
+    double t = fma(b.U, lm.x, fma(b.V, lm.y, fma(b.W, nd, b.C)));
+    unsigned lo = (unsigned)__double2loint(t);
+    unsigned kb = ((lo >> kFracShift) & 0x7FFFFFu) | 0x4B000000u;
+    float ang = __fmaf_rn(__uint_as_float(kb), kAngScale, -kTwoPiF);
+    __sincosf(ang, &s, &c);
+  } else if constexpr (MODE == VB_PREC_FP32_DSPH) {
+    float p1 = __fmul_rn(b.uf, f.x), e1 = __fmaf_rn(b.uf, f.x, -p1);
+    float p2 = __fmul_rn(b.vf, f.y), e2 = __fmaf_rn(b.vf, f.y, -p2);
+    float p3 = __fmul_rn(b.wf, f.z), e3 = __fmaf_rn(b.wf, f.z, -p3);
+    float f1 = __fsub_rn(p1, rint_magic(p1));
+    float f2 = __fsub_rn(p2, rint_magic(p2));
+    float f3 = __fsub_rn(p3, rint_magic(p3));
+    float sfr = __fadd_rn(__fadd_rn(f1, f2), __fadd_rn(f3, b.fw));
+    float efr = __fadd_rn(__fadd_rn(e1, e2), e3);
+    float t = __fadd_rn(sfr, efr);
+    t = __fsub_rn(t, rint_magic(t));
+    __sincosf(__fmul_rn(t, kTwoPiF), &s, &c);
+  } else if constexpr (MODE == VB_PREC_REF32) {
+    float ang = raw ? fmaf(b.kw, nm1, fmaf(b.kv, f.y, b.ku * f.x))
+                    : fmaf(b.kw, f.z, fmaf(b.kv, f.y, b.ku * f.x));
+    __sincosf(ang, &s, &c);
+  } else {  // FP64
+    double t = fma(b.U, lm.x, fma(b.V, lm.y, b.W * (raw ? (nd - 1.0) : nd)));
+    sincos(-6.283185307179586476925286766559 * t, &sd, &cd);
+  }
+}
+
+// Imaginary-part sign of the accumulated sums: F32X/DS accumulate sin(+2 pi t).
+template <int MODE>
+__device__ constexpr float imag_sign() {
+  return (MODE == VB_PREC_FP32_FP64PH || MODE == VB_PREC_FP32_DSPH) ? -1.0f : 1.0f;
+}
+
+template <int MODE, int BPT>
+__global__ void __launch_bounds__(S1_THREADS, 2) k_stage1(const S1Args a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double2* s_lm = reinterpret_cast<double2*>(smem_raw);
+  float4* s_nb = reinterpret_cast<float4*>(s_lm + a.stage_pix);
+  float4* s_f4 = s_nb + a.stage_pix;
+  __shared__ int s_item;
+  __shared__ unsigned long long s_cnt[4];
+
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  const bool raw = (a.phase_corrected == 0);
+  constexpr bool kDoubleAcc = (MODE == VB_PREC_FP64);
+
+  if (threadIdx.x < 4) s_cnt[threadIdx.x] = 0ull;
+
+  for (;;) {
+    __syncthreads();
+    if (threadIdx.x == 0) s_item = atomicAdd(a.queue, 1);
+    __syncthreads();
+    const int item = s_item;
+    if (item >= a.n_items) break;
+    const int btile = item / a.nchunk;
+    const int chunk = item - btile * a.nchunk;
+
+    // --- per-thread baselines -------------------------------------------------
+    Baseline bl[BPT];
+#pragma unroll
+    for (int k = 0; k < BPT; ++k) {
+      Baseline& b = bl[k];
+      const int ih = btile * (S1_THREADS * BPT) + warp * (32 * BPT) + k * 32 + lane;
+      load_baseline(a, ih, raw, b);
+      const float uu = b.uf, vv = b.vf, ww = b.wf;
+      if (MODE == VB_PREC_FP32_FP64PH && b.active &&
+          (fabsf(uu) >= (float)kMaxUvwF32X || fabsf(vv) >= (float)kMaxUvwF32X ||
+           fabsf(ww) >= (float)kMaxUvwF32X))
+        atomicOr(a.err, ERR_BAD_INDEX);
+    }
+
+    double accR[BPT], accI[BPT];
+    float kcR[BPT], kcI[BPT];   // Kahan compensation (DS)
+#pragma unroll
+    for (int k = 0; k < BPT; ++k) { accR[k] = 0.0; accI[k] = 0.0; kcR[k] = 0.f; kcI[k] = 0.f; }
+
+    unsigned long long cnt_fast = 0, cnt_mask = 0, cnt_hid = 0, cnt_all = 0;
+    int nact = 0;
+#pragma unroll
+    for (int k = 0; k < BPT; ++k) nact += __popc(__ballot_sync(0xffffffffu, bl[k].active));
+
+    const int64_t p_begin = (int64_t)chunk * a.chunk_pix;
+    int64_t p_end = p_begin + a.chunk_pix;
+    if (p_end > a.npix) p_end = a.npix;
+
+    for (int64_t t0 = p_begin; t0 < p_end; t0 += a.cull_tile) {
+      int64_t t1 = t0 + a.cull_tile;
+      if (t1 > p_end) t1 = p_end;
+      const int tile_id = (int)(t0 / a.cull_tile);
+
+      // --- tile classes of this thread's baselines ----------------------------
+      bool any_live = false, any_mix = false;
+#pragma unroll
+      for (int k = 0; k < BPT; ++k) {
+        Baseline& b = bl[k];
+        const int cls = tile_class(a, b, tile_id);
+        b.cls = cls;
+        any_live |= (cls != kClsHid);
+        any_mix |= (cls == kClsMix);
+      }
+      const bool warp_live = __any_sync(0xffffffffu, any_live);
+      const bool warp_mix = __any_sync(0xffffffffu, any_mix);
+      const int64_t tile_terms = (int64_t)nact * (t1 - t0);
+      cnt_all += tile_terms;
+      if (!warp_live) cnt_hid += tile_terms;
+      else if (warp_mix) cnt_mask += tile_terms;
+      else cnt_fast += tile_terms;
+
+      if (!__syncthreads_or(warp_live ? 1 : 0)) continue;
+
+      for (int64_t s0 = t0; s0 < t1; s0 += a.stage_pix) {
+        const int ns = (int)((t1 - s0) < a.stage_pix ? (t1 - s0) : a.stage_pix);
+        __syncthreads();
+        for (int j = threadIdx.x; j < ns; j += S1_THREADS) {
+          s_lm[j] = a.lm[s0 + j];
+          s_nb[j] = a.nb[s0 + j];
+          s_f4[j] = a.f4[s0 + j];
+        }
+        __syncthreads();
+        if (!warp_live) continue;
+
+        // two interleaved FP32 partial sums per baseline (even / odd pixels)
+        float pR0[BPT], pI0[BPT], pR1[BPT], pI1[BPT];
+        double dR[BPT], dI[BPT];
+#pragma unroll
+        for (int k = 0; k < BPT; ++k) {
+          pR0[k] = pI0[k] = pR1[k] = pI1[k] = 0.f;
+          dR[k] = dI[k] = 0.0;
+        }
+
+        // one pixel: MASKED selects the per-pixel occlusion test for mixed
+        // baselines (visible ones included unconditionally, hidden excluded)
+        auto pixel = [&](const int j, float (&aR)[BPT], float (&aI)[BPT], auto masked_tag) {
+          constexpr bool MASKED = decltype(masked_tag)::value;
+          const double2 lm = s_lm[j];
+          const float4 nb = s_nb[j];
+          const double nd = __hiloint2double(__float_as_int(nb.y), __float_as_int(nb.x));
+          float4 f;
+          if constexpr (MASKED || MODE == VB_PREC_FP32_DSPH || MODE == VB_PREC_REF32) f = s_f4[j];
+          else f = make_float4(0.f, 0.f, 0.f, nb.z);
+          const float Bp = nb.z;
+#pragma unroll
+          for (int k = 0; k < BPT; ++k) {
+            const Baseline& b = bl[k];
+            bool inc = true;
+            if constexpr (MASKED) {
+              const float o1 = occ_dot(f.x, f.y, f.z, b.x1, b.y1, b.z1, b.i1);
+              const float o2 = occ_dot(f.x, f.y, f.z, b.x2, b.y2, b.z2, b.i2);
+              const bool pass = !(o1 < b.c1 || o2 < b.c2);
+              inc = (b.cls == kClsVis) || (b.cls == kClsMix && pass);
+            }
+            float sn, cs;
+            double sd, cd;
+            phase_sincos<MODE>(b, lm, nd, f, nb.w, sn, cs, sd, cd, raw);
+            if constexpr (kDoubleAcc) {
+              const double Bw = inc ? (double)Bp : 0.0;
+              dR[k] = fma(Bw, cd, dR[k]);
+              dI[k] = fma(Bw, sd, dI[k]);
+            } else {
+              const float Bw = inc ? Bp : 0.0f;
+              aR[k] = fmaf(Bw, cs, aR[k]);
+              aI[k] = fmaf(Bw, sn, aI[k]);
+            }
+          }
+        };
+        using Unmasked = std::false_type;
+        using Masked = std::true_type;
+
+        int j = 0;
+        if (!warp_mix) {
+          for (; j + 1 < ns; j += 2) {
+            pixel(j, pR0, pI0, Unmasked{});
+            pixel(j + 1, pR1, pI1, Unmasked{});
+          }
+          if (j < ns) pixel(j, pR0, pI0, Unmasked{});
+        } else {
+          for (; j + 1 < ns; j += 2) {
+            pixel(j, pR0, pI0, Masked{});
+            pixel(j + 1, pR1, pI1, Masked{});
+          }
+          if (j < ns) pixel(j, pR0, pI0, Masked{});
+        }
+
+        // fold the staged-tile partials into the running totals
+#pragma unroll
+        for (int k = 0; k < BPT; ++k) {
+          if (bl[k].cls == kClsHid) continue;
+          if constexpr (kDoubleAcc) {
+            accR[k] += dR[k];
+            accI[k] += dI[k];
+          } else if constexpr (MODE == VB_PREC_FP32_DSPH) {
+            // Kahan summation in FP32 across staged tiles
+            float xr = __fadd_rn(pR0[k], pR1[k]);
+            float xi = __fadd_rn(pI0[k], pI1[k]);
+            float sr = (float)accR[k], si = (float)accI[k];
+            float yr = __fsub_rn(xr, kcR[k]);
+            float tr = __fadd_rn(sr, yr);
+            kcR[k] = __fsub_rn(__fsub_rn(tr, sr), yr);
+            float yi = __fsub_rn(xi, kcI[k]);
+            float ti = __fadd_rn(si, yi);
+            kcI[k] = __fsub_rn(__fsub_rn(ti, si), yi);
+            accR[k] = tr;
+            accI[k] = ti;
+          } else {
+            accR[k] += (double)pR0[k] + (double)pR1[k];
+            accI[k] += (double)pI0[k] + (double)pI1[k];
+          }
+        }
+      }
+    }
+
+#pragma unroll
+    for (int k = 0; k < BPT; ++k) {
+      const int ih = btile * (S1_THREADS * BPT) + warp * (32 * BPT) + k * 32 + lane;
+      if (ih < a.n_half)
+        a.partial[(int64_t)chunk * a.n_half + ih] =
+            make_double2(accR[k], (double)imag_sign<MODE>() * accI[k]);
+    }
+    if (a.counters && lane == 0) {
+      atomicAdd(&s_cnt[0], cnt_fast);
+      atomicAdd(&s_cnt[1], cnt_mask);
+      atomicAdd(&s_cnt[2], cnt_hid);
+      atomicAdd(&s_cnt[3], cnt_all);
+    }
+  }
+  __syncthreads();
+  if (a.counters && threadIdx.x < 4) atomicAdd(&a.counters[threadIdx.x], s_cnt[threadIdx.x]);
+}
+
+// V[ih] = sum over chunks of the partials, in chunk order.
+__global__ void k_reduce_partials(const double2* __restrict__ partial, int nchunk, int n_half,
+                                  double* __restrict__ V) {
+  for (int ih = blockIdx.x * blockDim.x + threadIdx.x; ih < n_half; ih += gridDim.x * blockDim.x) {
+    double r = 0.0, im = 0.0;
+    for (int c = 0; c < nchunk; ++c) {
+      double2 p = partial[(int64_t)c * n_half + ih];
+      r += p.x;
+      im += p.y;
+    }
+    V[2 * ih] = r;
+    V[2 * ih + 1] = im;
+  }
+}
+
+// V *= exp(-2 pi i w) in FP64 with the exact turn fraction of w, then FP32
+// half and conjugate-completed full layouts (common.hpp:255-277).
+__global__ void k_phase_correct_expand(const double* __restrict__ Vr, const float* __restrict__ w,
+                                       int n_half, int nbl, int already, float* __restrict__ Vh,
+                                       float* __restrict__ Vf) {
+  for (int ih = blockIdx.x * blockDim.x + threadIdx.x; ih < n_half; ih += gridDim.x * blockDim.x) {
+    const int ip = half_to_full_pos(ih, nbl);
+    double re = Vr[2 * ih], im = Vr[2 * ih + 1];
+    if (!already) {
+      double ww = (double)w[ip];
+      double fr = ww - rint(ww);
+      double s, c;
+      sincospi(-2.0 * fr, &s, &c);
+      double nr = re * c - im * s;
+      double ni = re * s + im * c;
+      re = nr;
+      im = ni;
+    }
+    float fr_ = (float)re, fi_ = (float)im;
+    if (Vh) { Vh[2 * ih] = fr_; Vh[2 * ih + 1] = fi_; }
+    if (Vf) {
+      Vf[2 * ip] = fr_;
+      Vf[2 * ip + 1] = fi_;
+      Vf[2 * (ip + nbl)] = fr_;
+      Vf[2 * (ip + nbl) + 1] = -fi_;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+template <int MODE, int BPT>
+static int launch_mode(const S1Args& a, int grid, size_t smem, cudaStream_t s) {
+  auto kern = k_stage1<MODE, BPT>;
+  VB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  kern<<<grid, S1_THREADS, smem, s>>>(a);
+  VB_LAUNCH_CHECK();
+  return VB_OK;
+}
+
+template <int MODE>
+static int launch_bpt(const S1Args& a, int bpt, int grid, size_t smem, cudaStream_t s) {
+  switch (bpt) {
+    case 1: return launch_mode<MODE, 1>(a, grid, smem, s);
+    case 2: return launch_mode<MODE, 2>(a, grid, smem, s);
+    case 4: return launch_mode<MODE, 4>(a, grid, smem, s);
+    default: return fail(VB_ERR_INVALID, "stage 1: bpt=%d (1, 2 or 4)", bpt);
+  }
+}
+
+template <int MODE, int BPT>
+static int occupancy_of(size_t smem) {
+  int n = 0;
+  auto kern = k_stage1<MODE, BPT>;
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 1;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, S1_THREADS, smem) != cudaSuccess) return 1;
+  return n < 1 ? 1 : n;
+}
+
+static int occupancy(int mode, int bpt, size_t smem) {
+#define VB_OCC(M)                                          \
+  switch (bpt) {                                          \
+    case 1: return occupancy_of<M, 1>(smem);              \
+    case 2: return occupancy_of<M, 2>(smem);              \
+    default: return occupancy_of<M, 4>(smem);             \
+  }
+  switch (mode) {
+    case VB_PREC_REF32: VB_OCC(VB_PREC_REF32);
+    case VB_PREC_FP64: VB_OCC(VB_PREC_FP64);
+    case VB_PREC_FP32_FP64PH: VB_OCC(VB_PREC_FP32_FP64PH);
+    default: VB_OCC(VB_PREC_FP32_DSPH);
+  }
+#undef VB_OCC
+}
+
+static bool is_pow2(int x) { return x > 0 && (x & (x - 1)) == 0; }
+
+int stage1_plan(const vb_sky* sky, const vb_baselines* bl, const vb_stage1_opts* o, Stage1Plan* p) {
+  if (!sky || !bl || !o || !p) return fail(VB_ERR_INVALID, "stage 1: null argument");
+  if (sky->npix <= 0) return fail(VB_ERR_INVALID, "stage 1: npix=%lld", (long long)sky->npix);
+  if (bl->nbl <= 0 || bl->n_full < 0 || bl->n_full % (2 * bl->nbl) != 0)
+    return fail(VB_ERR_INVALID, "stage 1: n_full=%d must be a multiple of 2*nbl=%d", bl->n_full, 2 * bl->nbl);
+  if (o->precision < VB_PREC_REF32 || o->precision > VB_PREC_FP32_DSPH)
+    return fail(VB_ERR_INVALID, "stage 1: precision=%d", o->precision);
+  if (o->cull < VB_CULL_NONE || o->cull > VB_CULL_EXACT) return fail(VB_ERR_INVALID, "stage 1: cull=%d", o->cull);
+  Stage1Plan q{};
+  q.precision = o->precision;
+  q.cull = o->blockage ? o->cull : VB_CULL_NONE;
+  q.phase_corrected = o->phase_corrected ? 1 : 0;
+  q.blockage = o->blockage ? 1 : 0;
+  q.bpt = o->bpt > 0 ? o->bpt : 2;
+  if (q.bpt != 1 && q.bpt != 2 && q.bpt != 4) return fail(VB_ERR_INVALID, "stage 1: bpt=%d", q.bpt);
+  q.npix = sky->npix;
+  q.n_half = bl->n_full / 2;
+  q.nbl = bl->nbl;
+
+  int stage = o->stage_pix > 0 ? o->stage_pix : 1024;
+  if (!is_pow2(stage) || stage < 32 || stage > 2048)
+    return fail(VB_ERR_INVALID, "stage 1: stage_pix=%d (power of two in [32, 2048])", stage);
+  if (q.cull == VB_CULL_TILECONE) {
+    if (!is_pow2(sky->tile_pix)) return fail(VB_ERR_INVALID, "stage 1: tile_pix=%d must be a power of two", sky->tile_pix);
+    if (!sky->cx || !sky->cy || !sky->cz || !sky->cosA || !sky->sinA)
+      return fail(VB_ERR_INVALID, "stage 1: tile-cone culling needs the tile meta arrays");
+    q.cull_tile = sky->tile_pix;
+    if (stage > q.cull_tile) stage = q.cull_tile;
+  } else if (q.cull == VB_CULL_EXACT) {
+    int et = o->exact_tile_pix > 0 ? o->exact_tile_pix : 1024;
+    if (!is_pow2(et) || et < 32) return fail(VB_ERR_INVALID, "stage 1: exact_tile_pix=%d", et);
+    q.cull_tile = et;
+    if (stage > et) stage = et;
+  } else {
+    q.cull_tile = stage;
+  }
+  q.stage_pix = stage;
+  q.ntile_cull = (int)ceil_div(q.npix, q.cull_tile);
+
+  const int per_tile = S1_THREADS * q.bpt;
+  q.n_btile = (int)ceil_div(q.n_half, per_tile);
+  size_t smem = (size_t)stage * 48;
+  int occ = occupancy(q.precision, q.bpt, smem);
+  int capacity = sm_count() * occ;
+  q.grid = capacity;
+  int64_t target_items = (int64_t)capacity * 12;
+  int64_t nchunk = q.n_btile > 0 ? ceil_div(target_items, q.n_btile) : 1;
+  int64_t max_chunks = ceil_div(q.npix, q.cull_tile);
+  if (nchunk > max_chunks) nchunk = max_chunks;
+  if (nchunk < 1) nchunk = 1;
+  int64_t chunk = ceil_div(ceil_div(q.npix, nchunk), q.cull_tile) * q.cull_tile;
+  if (o->chunk_pix > 0) {
+    if (o->chunk_pix % q.cull_tile != 0)
+      return fail(VB_ERR_INVALID, "stage 1: chunk_pix=%d must be a multiple of the cull tile %d", o->chunk_pix,
+                  q.cull_tile);
+    chunk = o->chunk_pix;
+  }
+  if (chunk > INT32_MAX) chunk = (INT32_MAX / q.cull_tile) * (int64_t)q.cull_tile;
+  q.chunk_pix = (int)chunk;
+  q.nchunk = (int)ceil_div(q.npix, q.chunk_pix);
+  int64_t items = (int64_t)q.n_btile * q.nchunk;
+  if (items > INT32_MAX) return fail(VB_ERR_UNSUPPORTED, "stage 1: too many work items");
+  q.n_items = (int)items;
+  if (q.grid > q.n_items) q.grid = q.n_items > 0 ? q.n_items : 1;
+  *p = q;
+  return VB_OK;
+}
+
+size_t stage1_carve(const Stage1Plan& p, void* ws, size_t cap, Stage1Buffers* b, bool pack_pixels) {
+  Carve c(ws, cap);
+  Stage1Buffers x;
+  if (pack_pixels) {
+    x.lm = c.take<double2>(p.npix);
+    x.nb = c.take<float4>(p.npix);
+    x.f4 = c.take<float4>(p.npix);
+    if (p.cull == VB_CULL_EXACT) x.cones = c.take<ExactCone>(p.ntile_cull);
+  }
+  x.partial = c.take<double2>((size_t)p.nchunk * (size_t)p.n_half);
+  x.queue = c.take<int>(4);
+  x.err = c.take<unsigned>(4);
+  if (b) *b = x;
+  if (ws && !c.ok) return 0;
+  return c.used();
+}
+
+int stage1_prepare_pixels(const vb_sky* sky, const Stage1Plan& p, const Stage1Buffers& b, cudaStream_t s) {
+  VB_TRY(geom_pack_pixels(sky->B, sky->l, sky->m, sky->n, p.npix, b.lm, b.nb, b.f4, s));
+  if (p.cull == VB_CULL_EXACT) VB_TRY(geom_exact_cones(p.cull_tile, sky->l, sky->m, sky->n, p.npix, b.cones, s));
+  return VB_OK;
+}
+
+int stage1_run(const vb_sky* sky, const vb_baselines* bl, const Stage1Plan& p, const Stage1Buffers& b,
+               bool pixels_ready, double* V_half, unsigned long long* counters, cudaStream_t s) {
+  if (p.n_half == 0) return VB_OK;
+  if (!pixels_ready) VB_TRY(stage1_prepare_pixels(sky, p, b, s));
+  S1Args a{};
+  a.lm = b.lm; a.nb = b.nb; a.f4 = b.f4;
+  a.npix = p.npix;
+  a.cull = p.cull; a.cull_tile = p.cull_tile; a.stage_pix = p.stage_pix; a.chunk_pix = p.chunk_pix;
+  a.nchunk = p.nchunk; a.n_btile = p.n_btile; a.n_items = p.n_items;
+  a.tcx = sky->cx; a.tcy = sky->cy; a.tcz = sky->cz; a.tcosA = sky->cosA; a.tsinA = sky->sinA;
+  a.cones = b.cones;
+  a.u = bl->u; a.v = bl->v; a.w = bl->w;
+  a.x1 = bl->x1; a.y1 = bl->y1; a.z1 = bl->z1; a.in1 = bl->invn1;
+  a.x2 = bl->x2; a.y2 = bl->y2; a.z2 = bl->z2; a.in2 = bl->invn2;
+  a.cp1 = bl->cosphi1; a.cp2 = bl->cosphi2; a.cosphi = bl->cosphi;
+  a.n_half = p.n_half; a.nbl = p.nbl; a.blockage = p.blockage; a.phase_corrected = p.phase_corrected;
+  a.queue = b.queue; a.partial = b.partial; a.counters = counters; a.err = b.err;
+  VB_CUDA(cudaMemsetAsync(b.queue, 0, sizeof(int), s));
+  size_t smem = (size_t)p.stage_pix * 48;
+  switch (p.precision) {
+    case VB_PREC_REF32: VB_TRY(launch_bpt<VB_PREC_REF32>(a, p.bpt, p.grid, smem, s)); break;
+    case VB_PREC_FP64: VB_TRY(launch_bpt<VB_PREC_FP64>(a, p.bpt, p.grid, smem, s)); break;
+    case VB_PREC_FP32_FP64PH: VB_TRY(launch_bpt<VB_PREC_FP32_FP64PH>(a, p.bpt, p.grid, smem, s)); break;
+    default: VB_TRY(launch_bpt<VB_PREC_FP32_DSPH>(a, p.bpt, p.grid, smem, s)); break;
+  }
+  int rg = (int)ceil_div(p.n_half, 256);
+  if (rg > sm_count() * 16) rg = sm_count() * 16;
+  k_reduce_partials<<<rg, 256, 0, s>>>(b.partial, p.nchunk, p.n_half, V_half);
+  VB_LAUNCH_CHECK();
+  return VB_OK;
+}
+
+int phase_correct_expand_async(const double* Vraw, const float* w_full, int n_half, int nbl, int already,
+                               float* Vh, float* Vf, cudaStream_t s) {
+  if (n_half <= 0) return VB_OK;
+  int g = (int)ceil_div(n_half, 256);
+  if (g > sm_count() * 16) g = sm_count() * 16;
+  k_phase_correct_expand<<<g, 256, 0, s>>>(Vraw, w_full, n_half, nbl, already, Vh, Vf);
+  VB_LAUNCH_CHECK();
+  return VB_OK;
+}
+
+}  // namespace vb
+
+using namespace vb;
+
+extern "C" size_t vb_stage1_workspace_bytes(const vb_sky* sky, const vb_baselines* bl, const vb_stage1_opts* o) {
+  Stage1Plan p;
+  if (stage1_plan(sky, bl, o, &p) != VB_OK) return 0;
+  return stage1_carve(p, nullptr, 0, nullptr, true);
+}
+
+extern "C" int vb_viss_halfsym(const vb_sky* sky, const vb_baselines* bl, const vb_stage1_opts* o, void* workspace,
+                               size_t ws_bytes, double* V_half, unsigned long long* term_counters, void* stream) {
+  Stage1Plan p;
+  VB_TRY(stage1_plan(sky, bl, o, &p));
+  if (p.n_half == 0) return VB_OK;
+  if (!V_half) return fail(VB_ERR_INVALID, "vb_viss_halfsym: V_half is NULL");
+  if (!sky->B || !sky->l || !sky->m || !sky->n) return fail(VB_ERR_INVALID, "vb_viss_halfsym: sky arrays missing");
+  if (!bl->u || !bl->v || !bl->w) return fail(VB_ERR_INVALID, "vb_viss_halfsym: u/v/w missing");
+  if (p.blockage && (!bl->x1 || !bl->y1 || !bl->z1 || !bl->invn1 || !bl->x2 || !bl->y2 || !bl->z2 || !bl->invn2))
+    return fail(VB_ERR_INVALID, "vb_viss_halfsym: endpoint arrays missing");
+  Stage1Buffers b;
+  size_t need = stage1_carve(p, nullptr, 0, nullptr, true);
+  if (!workspace || ws_bytes < need)
+    return fail(VB_ERR_NOMEM, "vb_viss_halfsym: workspace %zu bytes < %zu", ws_bytes, need);
+  stage1_carve(p, workspace, ws_bytes, &b, true);
+  cudaStream_t s = as_stream(stream);
+  VB_CUDA(cudaMemsetAsync(b.err, 0, sizeof(unsigned), s));
+  return stage1_run(sky, bl, p, b, false, V_half, term_counters, s);
+}
+
+extern "C" int vb_phase_correct_expand(const double* V_half_raw, const float* w_full, int n_half, int nbl,
+                                       int already_corrected, float* V_half_out, float* V_full_out, void* stream) {
+  if (n_half < 0 || nbl <= 0 || n_half % nbl != 0)
+    return fail(VB_ERR_INVALID, "vb_phase_correct_expand: n_half=%d nbl=%d", n_half, nbl);
+  if (n_half == 0) return VB_OK;
+  if (!V_half_raw || (!already_corrected && !w_full)) return fail(VB_ERR_INVALID, "vb_phase_correct_expand: null input");
+  return phase_correct_expand_async(V_half_raw, w_full, n_half, nbl, already_corrected, V_half_out, V_full_out,
+                                    as_stream(stream));
+}
+
+namespace vb {
+__global__ void k_tile_classes(const S1Args a, int ntile, uint8_t* __restrict__ cls) {
+  const bool raw = (a.phase_corrected == 0);
+  const int64_t total = (int64_t)a.n_half * ntile;
+  for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < total; q += (int64_t)gridDim.x * blockDim.x) {
+    const int ih = (int)(q / ntile);
+    const int t = (int)(q - (int64_t)ih * ntile);
+    Baseline b;
+    load_baseline(a, ih, raw, b);
+    cls[q] = (uint8_t)tile_class(a, b, t);
+  }
+}
+}  // namespace vb
+
+extern "C" int vb_stage1_tile_classes(const vb_sky* sky, const vb_baselines* bl, const vb_stage1_opts* o,
+                                      void* workspace, size_t ws_bytes, uint8_t* cls, int* ntile_out, void* stream) {
+  Stage1Plan p;
+  VB_TRY(stage1_plan(sky, bl, o, &p));
+  if (ntile_out) *ntile_out = p.ntile_cull;
+  if (p.n_half == 0) return VB_OK;
+  if (!cls) return fail(VB_ERR_INVALID, "vb_stage1_tile_classes: cls is NULL");
+  Stage1Buffers b;
+  size_t need = stage1_carve(p, nullptr, 0, nullptr, true);
+  if (!workspace || ws_bytes < need)
+    return fail(VB_ERR_NOMEM, "vb_stage1_tile_classes: workspace %zu bytes < %zu", ws_bytes, need);
+  stage1_carve(p, workspace, ws_bytes, &b, true);
+  cudaStream_t s = as_stream(stream);
+  if (p.cull == VB_CULL_EXACT)
+    VB_TRY(geom_exact_cones(p.cull_tile, sky->l, sky->m, sky->n, p.npix, b.cones, s));
+  S1Args a{};
+  a.npix = p.npix;
+  a.cull = p.cull; a.cull_tile = p.cull_tile;
+  a.tcx = sky->cx; a.tcy = sky->cy; a.tcz = sky->cz; a.tcosA = sky->cosA; a.tsinA = sky->sinA;
+  a.cones = b.cones;
+  a.u = bl->u; a.v = bl->v; a.w = bl->w;
+  a.x1 = bl->x1; a.y1 = bl->y1; a.z1 = bl->z1; a.in1 = bl->invn1;
+  a.x2 = bl->x2; a.y2 = bl->y2; a.z2 = bl->z2; a.in2 = bl->invn2;
+  a.cp1 = bl->cosphi1; a.cp2 = bl->cosphi2; a.cosphi = bl->cosphi;
+  a.n_half = p.n_half; a.nbl = p.nbl; a.blockage = p.blockage; a.phase_corrected = p.phase_corrected;
+  int64_t total = (int64_t)p.n_half * p.ntile_cull;
+  int g = (int)std::min<int64_t>(ceil_div(total, 256), (int64_t)sm_count() * 16);
+  k_tile_classes<<<g, 256, 0, s>>>(a, p.ntile_cull, cls);
+  VB_LAUNCH_CHECK();
+  return VB_OK;
+}
