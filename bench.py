@@ -1,0 +1,402 @@
+"""Benchmark of the two-stage direct-sum pipeline on B200.
+
+Metric: G pixel-baseline terms/s (stage 1 + stage 2), mixed precision, at
+<= 1e-5 relative error against the plain FP64 GPU build of the same pipeline.
+Nominal terms of one step = sum_seg npix * N_half,seg + sum_seg npix * nuniq_seg.
+
+Workload (one step = one whole day of the pipeline over resident inputs):
+nside 256 (786,432 HEALPix NESTED pixels), seeded synthetic sky (U[0,1) +
+20 point sources of amplitude 10), 10 MHz, 8 satellites on seeded circular
+orbits at 400-600 km over an Earth occluder (R = 6371 km), 28 baselines x
+1024 steps in 4 segments, tile-cone culling on nside-8 tiles (1024 pixels)
+with the all-visible fast path, mirrored half-grid occ_mode=2 reconstruction
+on a 513 x 513 uv grid, FP64-range-reduced phase with FP32 sincos/accumulate.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+N > 1 runs N independent replicas (one process per GPU, launched by
+torch.distributed.run): weak scaling, no data-path collective; the timed
+region is the max over ranks.  `--impl reference` times the CPU restatement
+of the upstream FP32 arithmetic (the upstream code has no CPU path) on this
+host's cores over a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "G pixel-baseline terms/s (viss+recon), mixed vs FP64 GPU, at ≤1e-5 rel err"
+UNIT = "Gterm/s"
+WORKLOAD = dict(workload="nside256_10MHz_8sat_1024steps_tilecone1024_mirror513_fp64phase", nside=256,
+                npix=786432, freq_mhz=10, nsat=8, baselines_per_step=28, tsteps=1024, segs=4,
+                tile_pix=1024, grid_res=513, mirror=1, occ_mode=2, precision="fp32_fp64phase",
+                occluder_R_km=6371.0, alt_km=[400, 600], sky="U[0,1)+20x10 seeded", sky_seed=1, orbit_seed=42)
+
+
+def workload_kwargs(prec: str = "fp32_fp64phase") -> dict:
+    import viss_optimize_ws_b200 as vb
+    return dict(nside=256, orbit_model=vb.ORBIT_SYNTHETIC, nsat=8, tsteps=1024, segs=4,
+                lambda_m=vb.btag_lambda("10M"), occ_R_m=6371e3, cull="tilecone", viss_tile_pix=1024, mirror=1,
+                grid_res=513, bl_max_m=100e3, orbit_seed=42, precision=prec, occ_mode=2, blockage=1)
+
+
+# ---------------------------------------------------------------------------
+def parse() -> argparse.Namespace:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 GPU comparison run")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    return ap.parse_args()
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class Dist:
+    """Barrier and max-reduction over ranks (torch.distributed, NCCL) or no-ops at N=1."""
+
+    def __init__(self, ws: int, local: int):
+        self.ws = ws
+        self.t = None
+        if ws > 1:
+            import datetime
+
+            import torch
+            import torch.distributed as td
+            torch.cuda.set_device(local)
+            td.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                  device_id=torch.device("cuda", local))
+            self.t, self.td, self.dev = torch, td, torch.device("cuda", local)
+
+    def barrier(self):
+        if self.t is not None:
+            self.td.barrier()
+
+    def max(self, x: float) -> float:
+        if self.t is None:
+            return x
+        v = self.t.tensor([x], dtype=self.t.float64, device=self.dev)
+        self.td.all_reduce(v, op=self.td.ReduceOp.MAX)
+        return float(v.item())
+
+    def close(self):
+        if self.t is not None:
+            self.td.destroy_process_group()
+
+
+class Clocks:
+    """nvidia-smi samples (200 ms) during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except FileNotFoundError:
+            self.p = None
+
+    def stop(self) -> dict:
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.flush()
+        rows = [r.split(",") for r in Path(self.f.name).read_text().strip().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx.append(float(r[2]))
+                for i, nm in enumerate(names):
+                    if r[5 + i].strip().lower() == "active":
+                        reasons.add(nm)
+            except (ValueError, IndexError):
+                continue
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def rel_errs(a, b) -> tuple[float, float]:
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    d = a - b
+    return (float(np.abs(d).max() / np.abs(b).max()), float(np.linalg.norm(d) / np.linalg.norm(b)))
+
+
+def traffic_from_profiles(kernel: str) -> float | None:
+    """DRAM bytes per launch of `kernel` recorded from an ncu capture in profiles/."""
+    for f in sorted((ROOT / "profiles").glob("*.txt")):
+        for line in f.read_text().splitlines():
+            if line.startswith(f"traffic_bytes_per_launch[{kernel}]:"):
+                try:
+                    return float(line.split(":", 1)[1].split()[0])
+                except ValueError:
+                    return None
+    return None
+
+
+# ---------------------------------------------------------------------------
+def cpu_sample(stage1_half: int = 64, stage2_pix: int = 1536, seed: int = 1) -> dict:
+    """Times the oracle's restatement of the upstream FP32 arithmetic on a
+    bounded sample of the workload: `stage1_half` half-baselines x all pixels
+    (stage 1) and `stage2_pix` pixels x all groups (stage 2), all host threads.
+    Inputs are generated on the CPU (FP64 geometry rounded to float)."""
+    from oracle import py as orp
+    L = orp.oracle()
+    nside, T, nsat = 256, 1024, 8
+    npix = 12 * nside * nside
+    lam = float(np.float32(np.float32(3e8) / np.float32(1e7)))
+    l64, m64, n64 = orp.nest_lmn_f64(nside)
+    l, m, n = (a.astype(np.float32) for a in (l64, m64, n64))
+    B = orp.make_sky(nside, seed)
+    B = (B.astype(np.float64) * (4 * np.pi / npix)).astype(np.float32)
+    bl = orp.syn_baselines(nsat, T, lam=lam)
+    nbl = bl["nbl"]
+    n_half = nbl * T
+    # the upstream global horizon is replaced by the Earth horizon at 500 km
+    cosphi = float(-np.sqrt(1 - (6371.0 / 6871.0) ** 2))
+    rng = np.random.default_rng(seed)
+    ih = np.sort(rng.choice(n_half, stage1_half, replace=False)).astype(np.int32)
+    V = np.zeros(2 * stage1_half)
+    P = orp.ptr
+    t0 = time.perf_counter()
+    L.or_stage1_subset(npix, P(B), P(l), P(m), P(n), nbl, *[P(bl[k]) for k in ("u", "v", "w", "x1", "y1", "z1",
+                                                                              "invn1", "x2", "y2", "z2", "invn2")],
+                       cosphi, 0, stage1_half, P(ih), P(V))
+    t1 = time.perf_counter() - t0
+    # stage 2 sample: mirror occ_mode=2 over all 4 segments
+    Vh = np.zeros(2 * n_half, np.float32)
+    Vh[0::2] = 1.0
+    seg_t0 = np.array([0, 256, 512, 768], np.int32)
+    seg_tl = np.array([256] * 4, np.int32)
+    pix = np.sort(rng.choice(npix, stage2_pix, replace=False)).astype(np.int64)
+    Cout = np.zeros(stage2_pix)
+    t0 = time.perf_counter()
+    L.or_stage2_subset(npix, P(l), P(m), P(n), nbl, 4, P(seg_t0), P(seg_tl),
+                       *[P(bl[k]) for k in ("u", "v", "w", "x1", "y1", "z1", "invn1", "x2", "y2", "z2", "invn2")],
+                       cosphi, P(Vh), 100e3, lam, 513, 0, stage2_pix, P(pix), P(Cout))
+    t2 = time.perf_counter() - t0
+    # groups per segment for the stage-2 term count
+    nuniq = 0
+    for s in range(4):
+        i0, nn = 2 * nbl * seg_t0[s], 2 * nbl * seg_tl[s]
+        fa, fb, _ = orp.fa_fb(bl["u"][i0:i0 + nn], bl["v"][i0:i0 + nn], bl["w"][i0:i0 + nn])
+        R, half, du = orp.grid_params(fa, fb, 100e3, lam, 513)
+        k = orp.keys(np.ascontiguousarray(bl["u"][i0:i0 + nn]), np.ascontiguousarray(bl["v"][i0:i0 + nn]), nn // 2,
+                     nbl, 1, float(np.float32(1) / np.float32(du)), R, half)
+        nuniq += int(np.unique(k).size)
+    terms = stage1_half * npix + stage2_pix * nuniq
+    return {"value": terms / (t1 + t2) / 1e9, "t_s": t1 + t2, "terms": terms, "cores": L.or_num_threads(),
+            "stage1_sample": f"{stage1_half} of {n_half} half-baselines x {npix} pixels",
+            "stage2_sample": f"{stage2_pix} of {npix} pixels x {nuniq} groups",
+            "full_step_terms_est": n_half * npix + npix * nuniq}
+
+
+def run_reference(args) -> None:
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return
+    steps, warm = args.steps, args.warmup
+    s1, s2 = 24, 512
+    for _ in range(max(0, warm)):
+        cpu_sample(s1, s2)
+    vals, tsum, terms = [], 0.0, 0
+    for _ in range(steps):
+        r = cpu_sample(s1, s2)
+        vals.append(r["value"])
+        tsum += r["t_s"]
+        terms += r["terms"]
+    value = terms / tsum / 1e9
+    sample = f"per step: {r['stage1_sample']} (stage 1) + {r['stage2_sample']} (stage 2)"
+    out = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": steps,
+           "warmup": warm, "ms_per_step": 1e3 * tsum / steps, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": WORKLOAD,
+           "cpu_baseline": {"value": value, "unit": UNIT, "cores": r["cores"], "kind": "port", "sample": sample},
+           "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+           "note": "upstream has no CPU implementation; this is the oracle's restatement of the upstream FP32 "
+                   "arithmetic (sincosf, FP32 sums, same masks and grouping), OpenMP over all host threads"}
+    print(json.dumps(out), flush=True)
+
+
+# ---------------------------------------------------------------------------
+def main() -> None:
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    import viss_optimize_ws_b200 as vb
+    ws, rank, local = dist_env()
+    dist = Dist(ws, local)
+    vb.check(vb.lib().vb_set_device(local))
+    L = vb.lib()
+
+    sfu, f32, f64, clk = (C.c_double() for _ in range(4))
+    vb.check(L.vb_measure_peaks(C.byref(sfu), C.byref(f32), C.byref(f64), C.byref(clk)))
+
+    B = vb.synthetic_sky(256, seed=1)
+    p = vb.Pipeline(vb.run_config(**workload_kwargs()))
+    p.set_sky(B)
+    p.make_baselines()
+    for _ in range(max(3, args.warmup)):
+        p.run()
+    flush = vb.DeviceBuffer(512 << 20)
+
+    clocks = Clocks(local)
+    clocks.start()
+    dist.barrier()
+    vb.check(L.vb_synchronize())
+    t_wall0 = time.perf_counter()
+    t_dev, t_k1, t_k2, reps = 0.0, 0.0, 0.0, []
+    for _ in range(args.steps):
+        vb.check(L.vb_flush_l2(flush.ptr, flush.nbytes, None))
+        vb.check(L.vb_synchronize())
+        r = p.run()
+        reps.append(r)
+        t_dev += r["t_stage1_ms"] + r["t_stage2_ms"]
+        t_k1 += r["t_s1_kernel_ms"]
+        t_k2 += r["t_s2_kernel_ms"]
+    vb.check(L.vb_synchronize())
+    dist.barrier()
+    t_wall = time.perf_counter() - t_wall0
+    clk_info = clocks.stop()
+    t_dev_max = dist.max(t_dev)
+
+    r = reps[-1]
+    terms_step = r["stage1_terms"] + r["stage2_terms"]
+    value = ws * terms_step * args.steps / (t_dev_max * 1e-3) / 1e9
+    ms_per_step = t_dev_max / args.steps
+
+    # end to end through the C ABI from pinned host buffers
+    npix = p.npix
+    hB = C.c_void_p()
+    hC = C.c_void_p()
+    hV = C.c_void_p()
+    vb.check(L.vb_host_alloc(C.byref(hB), 4 * npix))
+    vb.check(L.vb_host_alloc(C.byref(hC), 4 * npix))
+    vb.check(L.vb_host_alloc(C.byref(hV), 8 * p.n_half))
+    C.memmove(hB, B.ctypes.data, 4 * npix)
+    rep = vb.Report()
+    for _ in range(2):
+        vb.check(L.vb_pipeline_run_host(p.h, hB, 1, hC, hV, C.byref(rep)))
+    dist.barrier()
+    t_e2e = 0.0
+    e2e_steps = max(3, args.steps // 2)
+    for _ in range(e2e_steps):
+        vb.check(L.vb_flush_l2(flush.ptr, flush.nbytes, None))
+        vb.check(L.vb_synchronize())
+        vb.check(L.vb_pipeline_run_host(p.h, hB, 1, hC, hV, C.byref(rep)))
+        t_e2e += rep.t_e2e_ms
+    dist.barrier()
+    t_e2e_max = dist.max(t_e2e)
+    e2e_value = ws * terms_step * e2e_steps / (t_e2e_max * 1e-3) / 1e9
+    h2d = 4 * npix
+    d2h = 4 * npix + 8 * p.n_half
+    Cmixed = np.ctypeslib.as_array(C.cast(hC, C.POINTER(C.c_float)), shape=(npix,)).copy()
+    Vmixed = np.ctypeslib.as_array(C.cast(hV, C.POINTER(C.c_float)), shape=(2 * p.n_half,)).copy()
+
+    # plain FP64 GPU build of the same pipeline: speed and errors
+    fp64 = None
+    if not args.no_fp64:
+        q = vb.Pipeline(vb.run_config(**workload_kwargs("fp64")))
+        q.set_sky(B)
+        q.make_baselines()
+        q.run()
+        tq = []
+        for _ in range(2):
+            vb.check(L.vb_flush_l2(flush.ptr, flush.nbytes, None))
+            vb.check(L.vb_synchronize())
+            rq = q.run()
+            tq.append(rq["t_stage1_ms"] + rq["t_stage2_ms"])
+        V64, C64 = q.get("V_half"), q.get("C")
+        q.close()
+        ev = rel_errs(Vmixed, V64)
+        ec = rel_errs(Cmixed, C64)
+        t64 = dist.max(min(tq))
+        fp64 = {"value": ws * terms_step / (t64 * 1e-3) / 1e9, "ms_per_step": t64,
+                "speedup_mixed_vs_fp64": t64 / ms_per_step,
+                "error_vs_fp64": {"V_max": ev[0], "V_rms": ev[1], "C_max": ec[0], "C_rms": ec[1]}}
+    dist.barrier()
+
+    # roofline of the dominant kernel (stage 1): evaluated terms / kernel time
+    # against the measured SFU rate (one sin + one cos per term)
+    s1c, s2c = r["s1_counters"], r["s2_counters"]
+    k1_ms = t_k1 / args.steps
+    k2_ms = t_k2 / args.steps
+    s1_eval = s1c[0] + s1c[1]
+    s2_eval = s2c[0] + s2c[1]
+    peak_terms = sfu.value / 1e9          # G sincos pairs per second
+    ach1 = s1_eval / (k1_ms * 1e-3) / 1e9
+    ach2 = s2_eval / (k2_ms * 1e-3) / 1e9
+    traffic = traffic_from_profiles("k_stage1")
+    roofline = {"bound": "sfu", "kernel": "k_stage1", "achieved": ach1, "peak": peak_terms, "unit": "Gterm/s",
+                "frac": ach1 / peak_terms, "traffic": traffic,
+                "peak_source": "measured on this GPU by vb_measure_peaks (sin+cos pairs/s, MUFU)",
+                "per_unit": "1 evaluated term = 1 sin + 1 cos on the SFU (+ 3 DFMA phase, 2 FFMA accumulate)",
+                "units_per_launch": int(s1_eval), "kernel_ms": k1_ms,
+                "stage2": {"kernel": "k_recon_rec", "achieved": ach2, "frac": ach2 / peak_terms,
+                           "kernel_ms": k2_ms, "units_per_launch": int(s2_eval)},
+                "fp32_fma_per_s": f32.value, "fp64_fma_per_s": f64.value, "sm_clock_mhz_microbench": clk.value}
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        cs = cpu_sample()
+        cpu = {"value": cs["value"], "unit": UNIT, "cores": cs["cores"], "kind": "port",
+               "sample": f"{cs['stage1_sample']} (stage 1) + {cs['stage2_sample']} (stage 2); "
+                         f"oracle restatement of the upstream FP32 arithmetic"}
+
+    out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f32+f64phase", "data": "synthetic",
+           "config": dict(WORKLOAD, parallelism=f"replicas{ws}", l2="flushed between steps (512 MiB write)",
+                          terms_per_step=terms_step, stage1_terms=r["stage1_terms"], stage2_terms=r["stage2_terms"],
+                          groups=r["groups_total"]),
+           "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                   "ms_per_step": t_e2e_max / e2e_steps},
+           "gpu_launches": int(r["graph_kernels"]) * args.steps,
+           "roofline": roofline, "cpu_baseline": cpu, "fp64_gpu": fp64, "clocks": clk_info,
+           "wall_s_timed": t_wall, "counters": {"stage1": s1c, "stage2": s2c}}
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    vb.check(L.vb_host_free(hB))
+    vb.check(L.vb_host_free(hC))
+    vb.check(L.vb_host_free(hV))
+    p.close()
+    dist.close()
+
+
+if __name__ == "__main__":
+    main()

@@ -329,8 +329,11 @@ typedef struct {
   unsigned long long s1_counters[4];
   unsigned long long s2_counters[4];
   double   w_scalar_total; /* blockage=0 normaliser (sum nuniq) */
+  double   t_s1_kernel_ms; /* the stage-1 direct-sum kernel alone */
+  double   t_s2_kernel_ms; /* the stage-2 reconstruction kernel alone */
+  double   t_e2e_ms;       /* vb_pipeline_run_host: H2D, baselines, both stages, D2H */
   int      error_flags;    /* device-side error word (0 = ok) */
-  int      pad;
+  int      graph_kernels;  /* kernel nodes of the captured run graph (0 = eager) */
 } vb_report;
 
 void vb_run_config_defaults(vb_run_config* c);
@@ -389,6 +392,8 @@ int vb_flush_l2(void* buf, size_t bytes, void* stream);
 #define VB_D2H 1
 #define VB_D2D 2
 int vb_set_device(int device);
+int vb_host_alloc(void** ptr, size_t bytes);   /* page-locked host memory */
+int vb_host_free(void* ptr);
 int vb_malloc(void** ptr, size_t bytes);
 int vb_free(void* ptr);
 int vb_memcpy(void* dst, const void* src, size_t bytes, int kind);   /* synchronous */

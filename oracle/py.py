@@ -80,23 +80,68 @@ def ref_available() -> bool:
     return REF_ROOT_SO.exists() and REF_VF_SO.exists()
 
 
+def _sig(L, table):
+    for name, (res, args) in table.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+
+
+_P = C.c_void_p
+_I = C.c_int
+_F = C.c_float
+_LL = C.c_longlong
+
+
 def ref_root() -> C.CDLL:
+    """Upstream root variant (viss_recon_kernel.cuh, orbit_online.cuh, common.hpp)."""
     global _rr
     if _rr is None:
-        _rr = C.CDLL(str(REF_ROOT_SO))
-        for name in ("ref_pix2lmn", "ref_invnorm3", "ref_orbit", "ref_validate_halfsym", "ref_viss_halfsym",
-                     "ref_locg_full", "ref_groups_full", "ref_recon_blockage", "ref_recon_keys_avg",
-                     "ref_add_normalize"):
-            getattr(_rr, name).restype = C.c_int
-        _rr.ref_fa_fb.restype = None
-        _rr.ref_phase_correct_expand.restype = None
+        L = C.CDLL(str(REF_ROOT_SO))
+        _sig(L, {
+            "ref_pix2lmn": (_I, [_I, C.c_uint, _I, _P, _P, _P]),
+            "ref_invnorm3": (_I, [_P, _P, _P, _P, _I]),
+            "ref_orbit": (_I, [_F, _I, C.c_ulonglong, _I, _I] + [_P] * 10),
+            "ref_validate_halfsym": (_I, [_P, _P, _P, _I]),
+            "ref_viss_halfsym": (_I, [_P, _P, _P, _P, _LL] + [_P] * 11 + [_I, _F, _P]),
+            "ref_fa_fb": (None, [_P, _P, _P, _I, _P, _P, _P]),
+            "ref_phase_correct_expand": (None, [_P, _P, _I, _P, _P]),
+            "ref_locg_full": (_I, [_P, _P, _P, _I, _F, _I, _I]),
+            "ref_groups_full": (_I, [_P, _P, _P, _I, _F, _I, _I, _I, _P, _P, _P, _P, _P]),
+            "ref_recon_blockage": (_I, [_LL, _P, _P, _P, _P, _P, _P, _P] + [_P] * 8 + [_I, _I, _I, _F, _F, _F, _F,
+                                                                                       _I, _P, _P]),
+            "ref_recon_keys_avg": (_I, [_LL, _P, _P, _P, _P, _P, _I, _I, _I, _F, _F, _F, _P]),
+            "ref_add_normalize": (_I, [_P, _P, _LL]),
+            "ref_malloc": (_P, [C.c_size_t]),
+            "ref_free": (_I, [_P]),
+            "ref_h2d": (_I, [_P, _P, C.c_size_t]),
+            "ref_d2h": (_I, [_P, _P, C.c_size_t]),
+        })
+        _rr = L
     return _rr
 
 
 def ref_vf() -> C.CDLL:
+    """Upstream superset variant (mirror_tile_vissfast)."""
     global _rv
     if _rv is None:
-        _rv = C.CDLL(str(REF_VF_SO))
+        L = C.CDLL(str(REF_VF_SO))
+        _sig(L, {
+            "ref_vf_pix2lmn": (_I, [_I, C.c_uint, _I, _P, _P, _P]),
+            "ref_vf_nm1": (_I, [_P, _P, _LL]),
+            "ref_vf_tile_meta": (_I, [_I, _P, _P, _P, _LL, _P, _P, _P, _P, _P]),
+            "ref_vf_classify": (_I, [_P, _P, _P, _F, _I, _P, _P]),
+            "ref_vf_viss_tilecone": (_I, [_I, _P, _P, _P, _P, _P, _LL, _P, _P, _P, _P, _P, _I] + [_P] * 11
+                                     + [_I, _F, _P]),
+            "ref_vf_orbit": (_I, [_F, _I, C.c_ulonglong, _I, _I] + [_P] * 9),
+            "ref_vf_locg_half": (_I, [_P, _P, _P, _I, _F, _I, _I]),
+            "ref_vf_groups_half": (_I, [_P, _P, _P, _I, _F, _I, _I, _I, _I] + [_P] * 7),
+            "ref_vf_recon_rep": (_I, [_LL, _P, _P, _P, _P, _P, _P, _P, _I, _P] + [_P] * 8 + [_F, _F, _F, _P, _P]),
+            "ref_vf_recon_half": (_I, [_LL, _P, _P, _P, _P, _P, _P, _P] + [_P] * 8 + [_I, _I, _I, _F, _F, _F, _F,
+                                                                                      _I, _P, _P]),
+            "ref_vf_recon_keys_avg_half": (_I, [_LL, _P, _P, _P, _P, _P, _I, _I, _I, _F, _F, _F, _P]),
+        })
+        _rv = L
     return _rv
 
 

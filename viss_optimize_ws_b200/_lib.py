@@ -80,10 +80,11 @@ class Report(C.Structure):
                 ("stage1_terms", C.c_longlong), ("stage2_terms", C.c_longlong), ("groups_total", C.c_longlong),
                 ("t_stage1_ms", C.c_double), ("t_stage2_ms", C.c_double), ("t_orbit_ms", C.c_double),
                 ("s1_counters", C.c_ulonglong * 4), ("s2_counters", C.c_ulonglong * 4),
-                ("w_scalar_total", C.c_double), ("error_flags", C.c_int), ("pad", C.c_int)]
+                ("w_scalar_total", C.c_double), ("t_s1_kernel_ms", C.c_double), ("t_s2_kernel_ms", C.c_double),
+                ("t_e2e_ms", C.c_double), ("error_flags", C.c_int), ("graph_kernels", C.c_int)]
 
     def as_dict(self) -> dict:
-        d = {k: getattr(self, k) for k, _ in self._fields_ if k not in ("s1_counters", "s2_counters", "pad")}
+        d = {k: getattr(self, k) for k, _ in self._fields_ if k not in ("s1_counters", "s2_counters")}
         d["npix"] = (self.npix_hi << 31) | self.npix_lo
         d["s1_counters"] = list(self.s1_counters)
         d["s2_counters"] = list(self.s2_counters)
@@ -135,6 +136,8 @@ _SIGS = {
     "vb_measure_peaks": (C.c_int, [C.POINTER(C.c_double)] * 4),
     "vb_flush_l2": (C.c_int, [vp, C.c_size_t, vp]),
     "vb_set_device": (C.c_int, [C.c_int]),
+    "vb_host_alloc": (C.c_int, [C.POINTER(vp), C.c_size_t]),
+    "vb_host_free": (C.c_int, [vp]),
     "vb_malloc": (C.c_int, [C.POINTER(vp), C.c_size_t]),
     "vb_free": (C.c_int, [vp]),
     "vb_memcpy": (C.c_int, [vp, vp, C.c_size_t, C.c_int]),

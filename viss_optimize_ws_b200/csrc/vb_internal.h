@@ -67,7 +67,8 @@ int stage1_plan(const vb_sky* sky, const vb_baselines* bl, const vb_stage1_opts*
 size_t stage1_carve(const Stage1Plan& p, void* ws, size_t cap, Stage1Buffers* b, bool pack_pixels);
 // pixels_ready: lm/nb/f4 (and cones for VB_CULL_EXACT) already hold this sky.
 int stage1_run(const vb_sky* sky, const vb_baselines* bl, const Stage1Plan& p, const Stage1Buffers& b,
-               bool pixels_ready, double* V_half, unsigned long long* counters, cudaStream_t s);
+               bool pixels_ready, double* V_half, unsigned long long* counters, cudaStream_t s,
+               cudaEvent_t kbeg = nullptr, cudaEvent_t kend = nullptr);
 int stage1_prepare_pixels(const vb_sky* sky, const Stage1Plan& p, const Stage1Buffers& b, cudaStream_t s);
 int phase_correct_expand_async(const double* Vraw, const float* w_full, int n_half, int nbl,
                                int already_corrected, float* Vh, float* Vf, cudaStream_t s);
@@ -95,6 +96,7 @@ size_t stage2_workspace(const Stage2Plan& p, void* ws, size_t cap, void** slices
 int stage2_run(const vb_sky* sky, const vb_baselines* bl, const float* V_half, int nseg, const int* seg_t0,
                const int* seg_tlen, const Stage2Plan& p, void* ws, size_t cap, float* C, uint32_t* W,
                vb_seg_params* seg_params, unsigned long long* counters, double* w_scalar_total,
-               cudaStream_t s, const Stage2Pixels* pre);
+               cudaStream_t s, const Stage2Pixels* pre, cudaEvent_t kbeg = nullptr,
+               cudaEvent_t kend = nullptr);
 
 }  // namespace vb

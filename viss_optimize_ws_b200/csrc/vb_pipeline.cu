@@ -119,7 +119,8 @@ struct vb_pipeline {
   double* wsum = nullptr;
   unsigned long long* counters = nullptr;  // [0..3] stage 1, [4..7] stage 2
   // timing / graph
-  cudaEvent_t ev[6] = {};
+  cudaEvent_t ev[10] = {};
+  int graph_kernels = 0;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t gexec = nullptr;
   std::vector<void*> owned;
@@ -442,18 +443,18 @@ static int enqueue_stages(vb_pipeline* p) {
   vb_sky sky = sky_of(p);
   vb_baselines bl = bl_of(p);
   VB_CUDA(cudaMemsetAsync(p->counters, 0, 8 * sizeof(unsigned long long), p->s));
-  VB_CUDA(cudaEventRecord(p->ev[0], p->s));
-  VB_TRY(stage1_run(&sky, &bl, p->p1, p->b1, true, p->Vd, p->counters, p->s));
+  VB_CUDA(cudaEventRecordWithFlags(p->ev[0], p->s, cudaEventRecordExternal));
+  VB_TRY(stage1_run(&sky, &bl, p->p1, p->b1, true, p->Vd, p->counters, p->s, p->ev[5], p->ev[6]));
   VB_TRY(phase_correct_expand_async(p->Vd, p->w, p->n_half, p->nbl, 1, p->Vh, p->Vf, p->s));
-  VB_CUDA(cudaEventRecord(p->ev[1], p->s));
+  VB_CUDA(cudaEventRecordWithFlags(p->ev[1], p->s, cudaEventRecordExternal));
   Stage2Pixels pre;
   pre.lm = p->b1.lm;
   pre.nb = p->b1.nb;
   pre.f4 = p->b1.f4;
   pre.cones_ready = p->s2_cones_ready;
   VB_TRY(stage2_run(&sky, &bl, p->Vh, p->nseg, p->d_t0, p->d_tlen, p->p2, p->ws2, p->ws2_bytes, p->C, p->W,
-                    p->segp, p->counters + 4, p->wsum, p->s, &pre));
-  VB_CUDA(cudaEventRecord(p->ev[2], p->s));
+                    p->segp, p->counters + 4, p->wsum, p->s, &pre, p->ev[7], p->ev[8]));
+  VB_CUDA(cudaEventRecordWithFlags(p->ev[2], p->s, cudaEventRecordExternal));
   return VB_OK;
 }
 
@@ -469,6 +470,12 @@ static int fill_report(vb_pipeline* p, vb_report* r) {
   VB_CUDA(cudaEventElapsedTime(&t2, p->ev[1], p->ev[2]));
   r->t_stage1_ms = t1;
   r->t_stage2_ms = t2;
+  float k1 = 0.f, k2 = 0.f;
+  VB_CUDA(cudaEventElapsedTime(&k1, p->ev[5], p->ev[6]));
+  VB_CUDA(cudaEventElapsedTime(&k2, p->ev[7], p->ev[8]));
+  r->t_s1_kernel_ms = k1;
+  r->t_s2_kernel_ms = k2;
+  r->graph_kernels = p->graph_kernels;
   unsigned long long cnt[8];
   VB_CUDA(cudaMemcpy(cnt, p->counters, sizeof(cnt), cudaMemcpyDeviceToHost));
   for (int k = 0; k < 4; ++k) {
@@ -523,6 +530,17 @@ static int run_once(vb_pipeline* p) {
       if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture", __FILE__, __LINE__);
       p->graph = g;
       VB_CUDA(cudaGraphInstantiate(&p->gexec, g, 0));
+      size_t nn = 0;
+      VB_CUDA(cudaGraphGetNodes(g, nullptr, &nn));
+      std::vector<cudaGraphNode_t> nodes(nn);
+      VB_CUDA(cudaGraphGetNodes(g, nodes.data(), &nn));
+      int nk = 0;
+      for (auto nd : nodes) {
+        cudaGraphNodeType t;
+        VB_CUDA(cudaGraphNodeGetType(nd, &t));
+        if (t == cudaGraphNodeTypeKernel) ++nk;
+      }
+      p->graph_kernels = nk;
     }
     VB_CUDA(cudaGraphLaunch(p->gexec, p->s));
   } else {
@@ -546,7 +564,7 @@ extern "C" int vb_pipeline_run_host(vb_pipeline* p, const float* B_host, int sca
                                     float* V_half_host, vb_report* r) {
   if (!p || !C_host) return fail(VB_ERR_INVALID, "vb_pipeline_run_host: null argument");
   VB_CUDA(cudaSetDevice(p->cfg.device));
-  VB_CUDA(cudaEventRecord(p->ev[3], p->s));
+  VB_CUDA(cudaEventRecordWithFlags(p->ev[3], p->s, cudaEventRecordExternal));
   VB_TRY(set_sky_async(p, B_host, scale));
   VB_TRY(make_baselines_async(p));
   p->baselines_ready = true;
@@ -557,13 +575,13 @@ extern "C" int vb_pipeline_run_host(vb_pipeline* p, const float* B_host, int sca
   VB_CUDA(cudaMemcpyAsync(C_host, p->C, p->npix * sizeof(float), cudaMemcpyDeviceToHost, p->s));
   if (V_half_host)
     VB_CUDA(cudaMemcpyAsync(V_half_host, p->Vh, (size_t)2 * p->n_half * sizeof(float), cudaMemcpyDeviceToHost, p->s));
-  VB_CUDA(cudaEventRecord(p->ev[4], p->s));
+  VB_CUDA(cudaEventRecordWithFlags(p->ev[4], p->s, cudaEventRecordExternal));
   VB_CUDA(cudaStreamSynchronize(p->s));
   VB_TRY(fill_report(p, r));
   if (r) {
     float te = 0.f;
     VB_CUDA(cudaEventElapsedTime(&te, p->ev[3], p->ev[4]));
-    r->t_orbit_ms = te;   // whole end-to-end call (H2D, baselines, both stages, D2H)
+    r->t_e2e_ms = te;   // whole end-to-end call (H2D, baselines, both stages, D2H)
   }
   return VB_OK;
 }
@@ -727,6 +745,17 @@ extern "C" int vb_flush_l2(void* buf, size_t bytes, void* stream) {
 // ---------------------------------------------------------------------------
 extern "C" int vb_set_device(int device) {
   VB_CUDA(cudaSetDevice(device));
+  return VB_OK;
+}
+extern "C" int vb_host_alloc(void** ptr, size_t bytes) {
+  if (!ptr) return fail(VB_ERR_INVALID, "vb_host_alloc: null ptr");
+  *ptr = nullptr;
+  cudaError_t e = cudaMallocHost(ptr, bytes ? bytes : 1);
+  if (e != cudaSuccess) return fail(VB_ERR_NOMEM, "vb_host_alloc(%zu): %s", bytes, cudaGetErrorString(e));
+  return VB_OK;
+}
+extern "C" int vb_host_free(void* ptr) {
+  if (ptr) VB_CUDA(cudaFreeHost(ptr));
   return VB_OK;
 }
 extern "C" int vb_malloc(void** ptr, size_t bytes) {

@@ -546,7 +546,8 @@ int stage1_prepare_pixels(const vb_sky* sky, const Stage1Plan& p, const Stage1Bu
 }
 
 int stage1_run(const vb_sky* sky, const vb_baselines* bl, const Stage1Plan& p, const Stage1Buffers& b,
-               bool pixels_ready, double* V_half, unsigned long long* counters, cudaStream_t s) {
+               bool pixels_ready, double* V_half, unsigned long long* counters, cudaStream_t s, cudaEvent_t kbeg,
+               cudaEvent_t kend) {
   if (p.n_half == 0) return VB_OK;
   if (!pixels_ready) VB_TRY(stage1_prepare_pixels(sky, p, b, s));
   S1Args a{};
@@ -564,12 +565,14 @@ int stage1_run(const vb_sky* sky, const vb_baselines* bl, const Stage1Plan& p, c
   a.queue = b.queue; a.partial = b.partial; a.counters = counters; a.err = b.err;
   VB_CUDA(cudaMemsetAsync(b.queue, 0, sizeof(int), s));
   size_t smem = (size_t)p.stage_pix * 48;
+  if (kbeg) VB_CUDA(cudaEventRecordWithFlags(kbeg, s, cudaEventRecordExternal));
   switch (p.precision) {
     case VB_PREC_REF32: VB_TRY(launch_bpt<VB_PREC_REF32>(a, p.bpt, p.grid, smem, s)); break;
     case VB_PREC_FP64: VB_TRY(launch_bpt<VB_PREC_FP64>(a, p.bpt, p.grid, smem, s)); break;
     case VB_PREC_FP32_FP64PH: VB_TRY(launch_bpt<VB_PREC_FP32_FP64PH>(a, p.bpt, p.grid, smem, s)); break;
     default: VB_TRY(launch_bpt<VB_PREC_FP32_DSPH>(a, p.bpt, p.grid, smem, s)); break;
   }
+  if (kend) VB_CUDA(cudaEventRecordWithFlags(kend, s, cudaEventRecordExternal));
   int rg = (int)ceil_div(p.n_half, 256);
   if (rg > sm_count() * 16) rg = sm_count() * 16;
   k_reduce_partials<<<rg, 256, 0, s>>>(b.partial, p.nchunk, p.n_half, V_half);

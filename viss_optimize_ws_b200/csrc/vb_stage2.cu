@@ -722,7 +722,7 @@ __global__ void k_expand_half(const float* __restrict__ Vh, int n_half, int nbl,
 int stage2_run(const vb_sky* sky, const vb_baselines* bl, const float* V_half, int nseg, const int* seg_t0,
                const int* seg_tlen, const Stage2Plan& p, void* ws, size_t cap, float* C, uint32_t* W,
                vb_seg_params* seg_params_out, unsigned long long* counters, double* w_scalar_total, cudaStream_t st,
-               const Stage2Pixels* pre) {
+               const Stage2Pixels* pre, cudaEvent_t kbeg, cudaEvent_t kend) {
   S2Slices x;
   if (!carve2(p, ws, cap, &x)) return fail(VB_ERR_NOMEM, "stage 2: workspace too small (%zu bytes)", cap);
   const int n = p.n_keyed_total;
@@ -801,12 +801,17 @@ int stage2_run(const vb_sky* sky, const vb_baselines* bl, const float* V_half, i
     ra.counters = counters; ra.err = x.err;
     const bool members = p.blockage && p.occ_mode != 2;
     VB_CUDA(cudaMemsetAsync(x.queue, 0, sizeof(int), st));
+    if (kbeg) VB_CUDA(cudaEventRecordWithFlags(kbeg, st, cudaEventRecordExternal));
     switch (p.precision) {
       case VB_PREC_REF32: VB_TRY(launch_recon<VB_PREC_REF32>(ra, members, st)); break;
       case VB_PREC_FP64: VB_TRY(launch_recon<VB_PREC_FP64>(ra, members, st)); break;
       case VB_PREC_FP32_FP64PH: VB_TRY(launch_recon<VB_PREC_FP32_FP64PH>(ra, members, st)); break;
       default: VB_TRY(launch_recon<VB_PREC_FP32_DSPH>(ra, members, st)); break;
     }
+    if (kend) VB_CUDA(cudaEventRecordWithFlags(kend, st, cudaEventRecordExternal));
+  } else if (kbeg) {
+    VB_CUDA(cudaEventRecordWithFlags(kbeg, st, cudaEventRecordExternal));
+    VB_CUDA(cudaEventRecordWithFlags(kend, st, cudaEventRecordExternal));
   }
   // 9. finalize: sum the group-chunk partials, normalise
   int gf = (int)ceil_div(p.npix, 256);
