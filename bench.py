@@ -73,9 +73,10 @@ def dist_env():
 
 
 class Dist:
-    """Barrier and max-reduction over ranks (torch.distributed, NCCL) or no-ops at N=1."""
+    """Barrier and max-reduction over ranks (torch.distributed) or no-ops at N=1.
+    NCCL on GPUs; gloo (CPU tensors) when `backend="gloo"`."""
 
-    def __init__(self, ws: int, local: int):
+    def __init__(self, ws: int, local: int, backend: str | None = None, timeout_s: float = 120.0):
         self.ws = ws
         self.t = None
         if ws > 1:
@@ -83,10 +84,16 @@ class Dist:
 
             import torch
             import torch.distributed as td
-            torch.cuda.set_device(local)
-            td.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                  device_id=torch.device("cuda", local))
-            self.t, self.td, self.dev = torch, td, torch.device("cuda", local)
+            backend = backend or "nccl"
+            kw = {}
+            if backend == "nccl":
+                torch.cuda.set_device(local)
+                self.dev = torch.device("cuda", local)
+                kw["device_id"] = self.dev
+            else:
+                self.dev = torch.device("cpu")
+            td.init_process_group(backend, timeout=datetime.timedelta(seconds=timeout_s), **kw)
+            self.t, self.td = torch, td
 
     def barrier(self):
         if self.t is not None:
@@ -102,6 +109,12 @@ class Dist:
     def close(self):
         if self.t is not None:
             self.td.destroy_process_group()
+
+
+def replica_value(terms_step: float, steps: int, t_dev_ms_max: float, ws: int) -> float:
+    """Whole-job throughput (G terms/s) of `ws` replicas, each running `steps`
+    steps of `terms_step` terms, timed by the slowest rank."""
+    return ws * terms_step * steps / (t_dev_ms_max * 1e-3) / 1e9
 
 
 class Clocks:
@@ -297,7 +310,7 @@ def main() -> None:
 
     r = reps[-1]
     terms_step = r["stage1_terms"] + r["stage2_terms"]
-    value = ws * terms_step * args.steps / (t_dev_max * 1e-3) / 1e9
+    value = replica_value(terms_step, args.steps, t_dev_max, ws)
     ms_per_step = t_dev_max / args.steps
 
     # end to end through the C ABI from pinned host buffers

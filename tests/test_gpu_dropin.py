@@ -1,0 +1,93 @@
+"""The drop-in executables against the upstream executables (built from the
+upstream sources into oracle/_ref) with the flag set of the upstream
+parameter script (main_recon_online.sh), reduced to a small sky:
+identical uvw / xyza / xyzb files, identical per-segment plane fits, grid
+sizes and group counts, and V / C that agree to the upstream FP32 level."""
+from __future__ import annotations
+
+import re
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from conftest import ROOT, rel_err
+
+pytestmark = pytest.mark.gpu
+
+BIN = ROOT / "viss_optimize_ws_b200" / "bin"
+UP = ROOT / "oracle" / "_ref"
+
+
+def run(exe: Path, args: list[str], cwd: Path) -> subprocess.CompletedProcess:
+    r = subprocess.run([str(exe), *args], cwd=cwd, capture_output=True, text=True, timeout=600)
+    return r
+
+
+def seg_lines(out: str) -> list[tuple]:
+    rows = []
+    for line in out.splitlines():
+        if not (line.startswith("[seg ") or line.startswith("[day ")) or "segN=" not in line:
+            continue
+        d = dict(re.findall(r"(\w+)=([^\s\]\[]+)", line))
+        nu = d.get("nuniq", d.get("nuniq_halfgrid"))
+        rows.append((int(d["t0"]), int(d["segN"]), d["fa"], d["fb"], int(nu), int(d["RES"])))
+    return rows
+
+
+@pytest.mark.parametrize("variant", ["root", "vissfast"])
+def test_dropin_matches_upstream_executable(gpu, vb, tmp_path, variant):
+    sky = tmp_path / "sky"
+    exe = BIN / ("main_recon_online" if variant == "root" else "main_recon_online_mirror_tile_vissfast")
+    up = UP / exe.name
+    assert exe.exists() and up.exists()
+    common = ["--btag=1M", "--nside=32", "--segs=4", "--blockage=1", "--occ_mode=2", f"--sky_dir={sky}",
+              "--gpus=0", "--gen_gpu_index=0", "--B_mode=bin", "--orbit_seed=42", "--write_viss=1",
+              "--write_baseline_txt=1"]
+    if variant == "root":
+        common.append("--day=1")
+    else:
+        common += ["--day_start=1", "--day_count=1", "--C_mode=txt"]
+    mine, theirs = tmp_path / "mine", tmp_path / "up"
+    r1 = run(exe, common + [f"--out_dir={mine}/", "--sky_gen=5"], tmp_path)
+    assert r1.returncode == 0, r1.stderr
+    # upstream's vissfast build reads B_10M.bin / B.bin whatever the btag
+    data = (sky / "B_1M.bin").read_bytes()
+    (sky / "B_10M.bin").write_bytes(data)
+    (sky / "B.bin").write_bytes(data)
+    r2 = run(up, common + [f"--out_dir={theirs}/"], tmp_path)
+    assert r2.returncode == 0, r2.stderr
+    # identical generated baselines (text formatting of identical floats)
+    for f in ("uvw1day1M.txt", "xyza1day1M.txt", "xyzb1day1M.txt"):
+        if variant == "vissfast" and not (theirs / f).exists():
+            continue
+        assert (mine / f).read_bytes() == (theirs / f).read_bytes(), f
+    # identical per-segment plan numbers
+    a, b = seg_lines(r1.stdout), seg_lines(r2.stdout)
+    assert len(a) == len(b) == 4
+    assert a == b
+    # V and C to the upstream FP32 level
+    Vm = np.loadtxt(mine / "Viss1day1M.txt")
+    Vu = np.loadtxt(theirs / "Viss1day1M.txt")
+    assert Vm.shape == Vu.shape
+    ev = rel_err(Vu, Vm)
+    assert ev[0] < 1e-3 and ev[1] < 1e-3, ev
+    Cm = np.loadtxt(mine / "C1day1M.txt")
+    Cu = np.loadtxt(theirs / "C1day1M.txt")
+    ec = rel_err(Cu, Cm)
+    assert ec[0] < 5e-3 and ec[1] < 5e-3, ec
+
+
+def test_dropin_error_paths(tmp_path):
+    exe = BIN / "main_recon_online"
+    r = run(exe, ["--btag=7M"], tmp_path)
+    assert r.returncode == 1 and "ERROR --btag" in r.stderr
+    r = run(exe, ["--btag=1M", "--nside=8", f"--sky_dir={tmp_path}/none", f"--out_dir={tmp_path}/o/"], tmp_path)
+    assert r.returncode == 1 and "ERROR" in r.stderr
+    # short sky file -> error exit 1 (upstream: load_single_bin_exact size check)
+    (tmp_path / "s").mkdir()
+    np.zeros(100, np.float32).tofile(tmp_path / "s" / "B_1M.bin")
+    r = run(exe, ["--btag=1M", "--nside=8", f"--sky_dir={tmp_path}/s", "--B_mode=bin", f"--out_dir={tmp_path}/o/"],
+            tmp_path)
+    assert r.returncode == 1 and "ERROR reading B" in r.stderr

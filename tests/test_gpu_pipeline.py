@@ -40,6 +40,9 @@ def pipeline_tile_classes(vb, p):
     bl.n_full, bl.nbl, bl.cosphi = 2 * p.n_half, p.nbl, p.cosphi
     for k in ("u", "v", "w", "x1", "y1", "z1", "x2", "y2", "z2", "invn1", "invn2"):
         setattr(bl, k, p.ptr(k)[0])
+    c1, n1 = p.ptr("cosphi1")
+    if c1 and n1:                                   # per-endpoint horizon cosines
+        bl.cosphi1, bl.cosphi2 = c1, p.ptr("cosphi2")[0]
     cls, tile = tile_classes(sky, bl, cull=vb.CULL_TILECONE)
     return cls, tile
 

@@ -72,8 +72,9 @@ def test_mask_fma_order_matches_oracle(case, vb, orc):
     x, y, z, inv = (np.ascontiguousarray(h[k][idx]) for k in ("x1", "y1", "z1", "invn1"))
     ne = idx.size
     mk = zeros(ne * c["npix"], np.uint8)
-    vb.check(vb.lib().vb_occlusion_mask(c["dl"].ptr, c["dm"].ptr, c["dn"].ptr, c["npix"], dev(x).ptr, dev(y).ptr,
-                                        dev(z).ptr, dev(inv).ptr, None, c["cosphi"], ne, mk.ptr, None))
+    dx, dy, dz, di = dev(x), dev(y), dev(z), dev(inv)      # held alive across the call
+    vb.check(vb.lib().vb_occlusion_mask(c["dl"].ptr, c["dm"].ptr, c["dn"].ptr, c["npix"], dx.ptr, dy.ptr, dz.ptr,
+                                        di.ptr, None, c["cosphi"], ne, mk.ptr, None))
     mine = get(mk, np.uint8).reshape(ne, c["npix"])
     v0 = orc.occlusion_mask(c["l"], c["m"], c["n"], x, y, z, inv, c["cosphi"], variant=0)
     v1 = orc.occlusion_mask(c["l"], c["m"], c["n"], x, y, z, inv, c["cosphi"], variant=1)
@@ -229,8 +230,9 @@ def test_phase_correct_expand(case, vb, orc, ref):
     assert np.array_equal(Vf[2 * f + 1], -Vf[2 * (f + c["nbl"]) + 1])
     # upstream host correction (FP32 cos/sin of a large angle) agrees loosely
     rh, rf = np.zeros(2 * nh, np.float32), np.zeros(4 * nh, np.float32)
-    ref.ref_root().ref_phase_correct_expand(Vraw.astype(np.float32).ctypes.data, c["host"]["w"].ctypes.data, nh,
-                                            rh.ctypes.data, rf.ctypes.data)
+    v32 = Vraw.astype(np.float32)                            # held alive across the call
+    ref.ref_root().ref_phase_correct_expand(v32.ctypes.data, c["host"]["w"].ctypes.data, nh, rh.ctypes.data,
+                                            rf.ctypes.data)
     assert rel_err(rh, Oh)[0] < 1e-3
 
 
@@ -276,3 +278,44 @@ def test_point_source_analytic(gpu, vb):
         V, _ = stage1(sky, bl, precision=prec, cull=vb.CULL_NONE, blockage=0)
         z = V[0::2] + 1j * V[1::2]
         assert np.abs(z - ex).max() < tol, (prec, np.abs(z - ex).max())
+
+
+def decode_my_masks(c, vb, cull):
+    """Effective inclusion decided by the library's own stage-1 kernel (FP64
+    mode, u=v=w=0, B_p = 2^k on 16-pixel blocks)."""
+    npix, nh = c["npix"], c["n_full"] // 2
+    zero = zeros(c["n_full"])
+    Bblk = dev((2.0 ** np.arange(16)).astype(np.float32))
+    out = np.zeros((nh, npix), np.uint8)
+    d = c["d"]
+    bl = vb.Baselines()
+    bl.n_full, bl.nbl, bl.cosphi = c["n_full"], c["nbl"], c["cosphi"]
+    bl.u = bl.v = bl.w = zero.ptr
+    for k in ("x1", "y1", "z1", "invn1", "x2", "y2", "z2", "invn2"):
+        setattr(bl, k, d[k].ptr)
+    o = vb.Stage1Opts(precision=vb.PREC_FP64, cull=cull, phase_corrected=1, blockage=1)
+    sky = vb.Sky()
+    sky.npix = 16
+    sky.tile_pix = 256
+    sky.B = Bblk.ptr
+    need = vb.lib().vb_stage1_workspace_bytes(C.byref(sky), C.byref(bl), C.byref(o))
+    ws = zeros(need, np.uint8)
+    V = zeros(2 * nh, np.float64)
+    for p0 in range(0, npix, 16):
+        off = 4 * p0
+        sky.l, sky.m, sky.n = c["dl"].ptr + off, c["dm"].ptr + off, c["dn"].ptr + off
+        t = p0 // 256
+        sky.cx, sky.cy, sky.cz, sky.cosA, sky.sinA = (a.ptr + 4 * t for a in c["tiles"])
+        vb.check(vb.lib().vb_viss_halfsym(C.byref(sky), C.byref(bl), C.byref(o), ws.ptr, need, V.ptr, None, None))
+        vx = get(V, np.float64)[0::2].astype(np.int64)
+        for k in range(16):
+            out[:, p0 + k] = (vx >> k) & 1
+    return out
+
+
+@pytest.mark.parametrize("cull", ["none", "tilecone"])
+def test_library_kernel_masks_match_upstream(case, vb, ref, cull):
+    cm = vb.CULL_NONE if cull == "none" else vb.CULL_TILECONE
+    mine = decode_my_masks(case, vb, cm)
+    up = decode_upstream_masks(case, ref, "plain" if cull == "none" else "tilecone")
+    assert np.array_equal(mine, up), f"{int((mine != up).sum())} differing (baseline, pixel) decisions"

@@ -71,4 +71,15 @@ struct Carve {
 
 int sm_count();   // cached SM count of the current device
 
+// Records an event so that it also records when the work is replayed from a
+// CUDA graph: inside a stream capture it must be an external event node
+// (a plain record there only orders streams).
+inline cudaError_t record_event(cudaEvent_t e, cudaStream_t s) {
+  cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+  cudaError_t r = cudaStreamIsCapturing(s, &st);
+  if (r != cudaSuccess) return r;
+  if (st == cudaStreamCaptureStatusActive) return cudaEventRecordWithFlags(e, s, cudaEventRecordExternal);
+  return cudaEventRecord(e, s);
+}
+
 }  // namespace vb

@@ -443,10 +443,10 @@ static int enqueue_stages(vb_pipeline* p) {
   vb_sky sky = sky_of(p);
   vb_baselines bl = bl_of(p);
   VB_CUDA(cudaMemsetAsync(p->counters, 0, 8 * sizeof(unsigned long long), p->s));
-  VB_CUDA(cudaEventRecordWithFlags(p->ev[0], p->s, cudaEventRecordExternal));
+  VB_CUDA(record_event(p->ev[0], p->s));
   VB_TRY(stage1_run(&sky, &bl, p->p1, p->b1, true, p->Vd, p->counters, p->s, p->ev[5], p->ev[6]));
   VB_TRY(phase_correct_expand_async(p->Vd, p->w, p->n_half, p->nbl, 1, p->Vh, p->Vf, p->s));
-  VB_CUDA(cudaEventRecordWithFlags(p->ev[1], p->s, cudaEventRecordExternal));
+  VB_CUDA(record_event(p->ev[1], p->s));
   Stage2Pixels pre;
   pre.lm = p->b1.lm;
   pre.nb = p->b1.nb;
@@ -454,7 +454,7 @@ static int enqueue_stages(vb_pipeline* p) {
   pre.cones_ready = p->s2_cones_ready;
   VB_TRY(stage2_run(&sky, &bl, p->Vh, p->nseg, p->d_t0, p->d_tlen, p->p2, p->ws2, p->ws2_bytes, p->C, p->W,
                     p->segp, p->counters + 4, p->wsum, p->s, &pre, p->ev[7], p->ev[8]));
-  VB_CUDA(cudaEventRecordWithFlags(p->ev[2], p->s, cudaEventRecordExternal));
+  VB_CUDA(record_event(p->ev[2], p->s));
   return VB_OK;
 }
 
@@ -564,7 +564,7 @@ extern "C" int vb_pipeline_run_host(vb_pipeline* p, const float* B_host, int sca
                                     float* V_half_host, vb_report* r) {
   if (!p || !C_host) return fail(VB_ERR_INVALID, "vb_pipeline_run_host: null argument");
   VB_CUDA(cudaSetDevice(p->cfg.device));
-  VB_CUDA(cudaEventRecordWithFlags(p->ev[3], p->s, cudaEventRecordExternal));
+  VB_CUDA(record_event(p->ev[3], p->s));
   VB_TRY(set_sky_async(p, B_host, scale));
   VB_TRY(make_baselines_async(p));
   p->baselines_ready = true;
@@ -575,7 +575,7 @@ extern "C" int vb_pipeline_run_host(vb_pipeline* p, const float* B_host, int sca
   VB_CUDA(cudaMemcpyAsync(C_host, p->C, p->npix * sizeof(float), cudaMemcpyDeviceToHost, p->s));
   if (V_half_host)
     VB_CUDA(cudaMemcpyAsync(V_half_host, p->Vh, (size_t)2 * p->n_half * sizeof(float), cudaMemcpyDeviceToHost, p->s));
-  VB_CUDA(cudaEventRecordWithFlags(p->ev[4], p->s, cudaEventRecordExternal));
+  VB_CUDA(record_event(p->ev[4], p->s));
   VB_CUDA(cudaStreamSynchronize(p->s));
   VB_TRY(fill_report(p, r));
   if (r) {

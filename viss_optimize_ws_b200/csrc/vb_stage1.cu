@@ -565,14 +565,14 @@ int stage1_run(const vb_sky* sky, const vb_baselines* bl, const Stage1Plan& p, c
   a.queue = b.queue; a.partial = b.partial; a.counters = counters; a.err = b.err;
   VB_CUDA(cudaMemsetAsync(b.queue, 0, sizeof(int), s));
   size_t smem = (size_t)p.stage_pix * 48;
-  if (kbeg) VB_CUDA(cudaEventRecordWithFlags(kbeg, s, cudaEventRecordExternal));
+  if (kbeg) VB_CUDA(record_event(kbeg, s));
   switch (p.precision) {
     case VB_PREC_REF32: VB_TRY(launch_bpt<VB_PREC_REF32>(a, p.bpt, p.grid, smem, s)); break;
     case VB_PREC_FP64: VB_TRY(launch_bpt<VB_PREC_FP64>(a, p.bpt, p.grid, smem, s)); break;
     case VB_PREC_FP32_FP64PH: VB_TRY(launch_bpt<VB_PREC_FP32_FP64PH>(a, p.bpt, p.grid, smem, s)); break;
     default: VB_TRY(launch_bpt<VB_PREC_FP32_DSPH>(a, p.bpt, p.grid, smem, s)); break;
   }
-  if (kend) VB_CUDA(cudaEventRecordWithFlags(kend, s, cudaEventRecordExternal));
+  if (kend) VB_CUDA(record_event(kend, s));
   int rg = (int)ceil_div(p.n_half, 256);
   if (rg > sm_count() * 16) rg = sm_count() * 16;
   k_reduce_partials<<<rg, 256, 0, s>>>(b.partial, p.nchunk, p.n_half, V_half);

@@ -801,17 +801,17 @@ int stage2_run(const vb_sky* sky, const vb_baselines* bl, const float* V_half, i
     ra.counters = counters; ra.err = x.err;
     const bool members = p.blockage && p.occ_mode != 2;
     VB_CUDA(cudaMemsetAsync(x.queue, 0, sizeof(int), st));
-    if (kbeg) VB_CUDA(cudaEventRecordWithFlags(kbeg, st, cudaEventRecordExternal));
+    if (kbeg) VB_CUDA(record_event(kbeg, st));
     switch (p.precision) {
       case VB_PREC_REF32: VB_TRY(launch_recon<VB_PREC_REF32>(ra, members, st)); break;
       case VB_PREC_FP64: VB_TRY(launch_recon<VB_PREC_FP64>(ra, members, st)); break;
       case VB_PREC_FP32_FP64PH: VB_TRY(launch_recon<VB_PREC_FP32_FP64PH>(ra, members, st)); break;
       default: VB_TRY(launch_recon<VB_PREC_FP32_DSPH>(ra, members, st)); break;
     }
-    if (kend) VB_CUDA(cudaEventRecordWithFlags(kend, st, cudaEventRecordExternal));
+    if (kend) VB_CUDA(record_event(kend, st));
   } else if (kbeg) {
-    VB_CUDA(cudaEventRecordWithFlags(kbeg, st, cudaEventRecordExternal));
-    VB_CUDA(cudaEventRecordWithFlags(kend, st, cudaEventRecordExternal));
+    VB_CUDA(record_event(kbeg, st));
+    VB_CUDA(record_event(kend, st));
   }
   // 9. finalize: sum the group-chunk partials, normalise
   int gf = (int)ceil_div(p.npix, 256);
