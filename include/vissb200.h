@@ -202,6 +202,26 @@ int vb_viss_halfsym(const vb_sky* sky, const vb_baselines* bl,
                     const vb_stage1_opts* o, void* workspace, size_t ws_bytes,
                     double* V_half, unsigned long long* term_counters, void* stream);
 
+/* Largest scratch of vb_viss_halfsym_noalloc, in bytes (64 MiB). */
+#define VB_VISS_NOALLOC_MAX_BYTES (64u << 20)
+
+/* vb_viss_halfsym for callers that cannot allocate device memory: code that
+ * runs while a stream is being captured into a CUDA graph, hosts whose device
+ * memory belongs to another allocator with a fixed budget, real-time loops.
+ * The caller passes only inputs and outputs.  No counterpart in the upstream
+ * project (upstream allocates everything in main()).
+ * Scratch is one file-scope device array of VB_VISS_NOALLOC_MAX_BYTES that
+ * every GPU which loads the library holds until the process exits; a sky /
+ * baseline set that needs more (about npix * 48 bytes + partial sums, e.g.
+ * nside >= 512) returns VB_ERR_UNSUPPORTED.  The first call on a device looks
+ * up the array's device address, so make that first call before any stream
+ * capture.  All calls share the one array and it keeps the last call's
+ * contents: calls that overlap on the GPU (other streams or threads) race.
+ * No cudaMalloc, cudaFree or allocating library routine is called. */
+int vb_viss_halfsym_noalloc(const vb_sky* sky, const vb_baselines* bl,
+                            const vb_stage1_opts* o, double* V_half,
+                            unsigned long long* term_counters, void* stream);
+
 /* Phase correction V *= exp(-2 pi i w) (skipped when already_corrected) in
  * FP64, then float32 outputs: V_half_out (2*n_half floats) and, if non-NULL,
  * the conjugate-completed signed layout V_full_out (4*n_half floats).

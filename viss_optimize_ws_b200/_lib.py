@@ -110,6 +110,8 @@ _SIGS = {
     "vb_stage1_workspace_bytes": (C.c_size_t, [C.POINTER(Sky), C.POINTER(Baselines), C.POINTER(Stage1Opts)]),
     "vb_viss_halfsym": (C.c_int, [C.POINTER(Sky), C.POINTER(Baselines), C.POINTER(Stage1Opts), vp, C.c_size_t,
                                   vp, vp, vp]),
+    "vb_viss_halfsym_noalloc": (C.c_int, [C.POINTER(Sky), C.POINTER(Baselines), C.POINTER(Stage1Opts), vp, vp,
+                                          vp]),
     "vb_stage1_tile_classes": (C.c_int, [C.POINTER(Sky), C.POINTER(Baselines), C.POINTER(Stage1Opts), vp,
                                          C.c_size_t, vp, C.POINTER(C.c_int), vp]),
     "vb_phase_correct_expand": (C.c_int, [vp, vp, C.c_int, C.c_int, C.c_int, vp, vp, vp]),

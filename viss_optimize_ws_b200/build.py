@@ -33,7 +33,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CUFLAGS = ["-O3", "--use_fast_math", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC",
            "-I", str(INCLUDE), "-I", str(CSRC)]
 
-LIB_SOURCES = ["vb_geom.cu", "vb_stage1.cu", "vb_stage2.cu", "vb_pipeline.cu"]
+LIB_SOURCES = ["vb_geom.cu", "vb_stage1.cu", "vb_stage2.cu", "vb_pipeline.cu", "vb_noalloc.cu"]
 EXE_SOURCES = ["main_recon_online.cpp"]
 
 
