@@ -57,7 +57,7 @@ def workload_kwargs(prec: str = "fp32_fp64phase") -> dict:
 def parse() -> argparse.Namespace:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 GPU comparison run")
@@ -125,17 +125,30 @@ class Clocks:
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, index: int):
-        self.index = index
+        # nvidia-smi numbers GPUs physically; CUDA_VISIBLE_DEVICES (indices or
+        # UUIDs, both accepted by --id) maps this process's device onto them
+        self.id = str(index)
+        vis = [x.strip() for x in os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",") if x.strip()]
+        if index < len(vis):
+            self.id = vis[index]
         self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
         self.p = None
 
     def start(self):
         try:
-            self.p = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={self.id}", f"--query-gpu={self.Q}",
                                        "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
                                       stderr=subprocess.DEVNULL)
         except FileNotFoundError:
             self.p = None
+            return
+        # nvidia-smi takes up to a second to print its first row: wait for it so
+        # that the samples cover the timed region
+        t0 = time.perf_counter()
+        while time.perf_counter() - t0 < 10.0 and self.p.poll() is None:
+            if Path(self.f.name).stat().st_size > 0:
+                break
+            time.sleep(0.05)
 
     def stop(self) -> dict:
         if self.p is None:
@@ -147,6 +160,7 @@ class Clocks:
             self.p.kill()
         self.f.flush()
         rows = [r.split(",") for r in Path(self.f.name).read_text().strip().splitlines() if r.strip()]
+        rows = rows[1:] if len(rows) > 1 else rows   # the first row predates the timed region
         os.unlink(self.f.name)
         sm, mx, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]

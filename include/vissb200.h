@@ -261,7 +261,7 @@ typedef struct {
   int grid_res;         /* > 0 forces RES */
   float bl_max;         /* metres */
   float lambda;         /* metres */
-  int ppt;              /* pixels per thread: 1 or 2 (0 = auto) */
+  int ppt;              /* pixels per thread of the occ_mode=2 / blockage=0 path: 1, 2 or 4 (0 = 2) */
 } vb_stage2_opts;
 
 typedef struct {       /* per-segment plane-fit and grid numbers, device or host copy */
@@ -331,6 +331,7 @@ typedef struct {
   int      seg_min_half, seg_max_half;  /* seg_plan=1: half-baseline count range per segment */
   uint64_t seg_seed;
   int      stage2_cull;    /* 2: exact pixel-block culling in stage 2, 0: off */
+  int      stage2_ppt;     /* stage-2 pixels per thread (vb_stage2_opts.ppt; 0 = auto) */
   int      use_graph;      /* 1: capture stages in one CUDA graph */
   int      device;         /* CUDA device ordinal */
 } vb_run_config;

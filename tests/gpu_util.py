@@ -154,11 +154,11 @@ def tile_classes(sky, bls, *, cull, precision=vb.PREC_FP32_FP64PH, exact_tile_pi
 
 
 def stage2(sky, bls, V_half_dev, seg_t0, seg_tlen, *, mirror=1, blockage=1, occ_mode=2, precision=2, cull=0,
-           grid_res=0, bl_max=100e3, lam=30.0):
+           grid_res=0, bl_max=100e3, lam=30.0, ppt=0):
     """vb_recon_batched on device inputs; returns C, W, per-segment params, counters."""
     nseg = len(seg_t0)
     o = vb.Stage2Opts(mirror=mirror, blockage=blockage, occ_mode=occ_mode, precision=precision, cull=cull,
-                      grid_res=grid_res, bl_max=bl_max, lambda_=lam)
+                      grid_res=grid_res, bl_max=bl_max, lambda_=lam, ppt=ppt)
     need = vb.lib().vb_stage2_workspace_bytes(bls.n_full // 2, nseg, sky.npix, C.byref(o))
     assert need > 0, vb.lib().vb_last_error()
     ws = DeviceBuffer(need)

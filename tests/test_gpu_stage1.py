@@ -298,6 +298,8 @@ def decode_my_masks(c, vb, cull):
     sky.npix = 16
     sky.tile_pix = 256
     sky.B = Bblk.ptr
+    sky.l, sky.m, sky.n = c["dl"].ptr, c["dm"].ptr, c["dn"].ptr
+    sky.cx, sky.cy, sky.cz, sky.cosA, sky.sinA = (a.ptr for a in c["tiles"])
     need = vb.lib().vb_stage1_workspace_bytes(C.byref(sky), C.byref(bl), C.byref(o))
     ws = zeros(need, np.uint8)
     V = zeros(2 * nh, np.float64)

@@ -159,16 +159,36 @@ def test_recon_vs_fp64_oracle(case, vb, orc, mirror, blockage, occ, prec):
     assert emax <= tol and erms <= tol, f"max {emax:.3e} rms {erms:.3e}"
 
 
-def test_recon_exact_block_culling_bit_identical(case, vb):
+@pytest.mark.parametrize("ppt", [1, 2, 4])
+def test_recon_exact_block_culling_bit_identical(case, vb, ppt):
+    """Exact pixel-block culling changes which groups take the per-pixel test,
+    never a result: C and W bit-identical to the unculled run at every block
+    size (256 * ppt pixels)."""
     c = case
+    proven = 0
     for pm in (vb.PREC_FP32_FP64PH, vb.PREC_FP32_DSPH, vb.PREC_FP64):
         C0, W0, _, k0 = stage2(c["sky"], c["bls"], c["dVh"], c["seg_t0"], c["seg_tlen"], precision=pm, cull=0,
-                               lam=LAM, bl_max=BL_MAX)
+                               lam=LAM, bl_max=BL_MAX, ppt=ppt)
         C1, W1, _, k1 = stage2(c["sky"], c["bls"], c["dVh"], c["seg_t0"], c["seg_tlen"], precision=pm, cull=2,
-                               lam=LAM, bl_max=BL_MAX)
+                               lam=LAM, bl_max=BL_MAX, ppt=ppt)
         assert np.array_equal(W0, W1)
         assert np.array_equal(C0.view(np.uint32), C1.view(np.uint32))
-        assert int(k1[0]) + int(k1[2]) > 0      # some blocks proven visible or hidden
+        assert int(k1[3]) == int(k0[3]) and int(k1[0] + k1[1] + k1[2]) == int(k1[3])
+        proven += int(k1[0]) + int(k1[2]) - int(k0[2])
+    if ppt == 1:
+        assert proven > 0      # 256-pixel blocks: some groups proven visible or hidden
+
+
+@pytest.mark.parametrize("ppt", [1, 2, 4])
+def test_recon_pixels_per_thread_vs_fp64_oracle(case, vb, orc, ppt):
+    c = case
+    Cd, W, params, cnt = stage2(c["sky"], c["bls"], c["dVh"], c["seg_t0"], c["seg_tlen"], precision=vb.PREC_FP32_FP64PH,
+                                cull=2, lam=LAM, bl_max=BL_MAX, ppt=ppt)
+    Co, Wo, sp = orc.stage2(c["skyh"], c["bl"], c["Vh"], c["seg_t0"], c["seg_tlen"], mirror=1, blockage=1,
+                            occ_mode=2, bl_max=BL_MAX, lam=LAM, precision=1)
+    assert np.array_equal(W, Wo)
+    emax, erms = rel_err(Cd, Co)
+    assert emax <= TOL and erms <= TOL, f"max {emax:.3e} rms {erms:.3e}"
 
 
 def test_recon_vs_upstream_rep_kernel(case, vb, orc, ref):

@@ -72,7 +72,7 @@ class RunConfig(C.Structure):
                 ("alt_min_km", C.c_double), ("alt_max_km", C.c_double), ("spread_km", C.c_double),
                 ("occ_R_m", C.c_double), ("bl_max_m", C.c_float), ("grid_res", C.c_int), ("seg_plan", C.c_int),
                 ("seg_min_half", C.c_int), ("seg_max_half", C.c_int), ("seg_seed", C.c_uint64),
-                ("stage2_cull", C.c_int), ("use_graph", C.c_int), ("device", C.c_int)]
+                ("stage2_cull", C.c_int), ("stage2_ppt", C.c_int), ("use_graph", C.c_int), ("device", C.c_int)]
 
 
 class Report(C.Structure):

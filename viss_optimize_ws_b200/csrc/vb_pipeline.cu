@@ -374,6 +374,7 @@ extern "C" int vb_pipeline_create(const vb_run_config* c, vb_pipeline** out) {
   o2.occ_mode = c->occ_mode;
   o2.precision = c->precision;
   o2.cull = c->stage2_cull;
+  o2.ppt = c->stage2_ppt;
   o2.grid_res = c->grid_res;
   o2.bl_max = c->bl_max_m;
   o2.lambda = c->lambda_m;

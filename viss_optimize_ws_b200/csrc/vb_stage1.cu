@@ -128,13 +128,24 @@ __device__ __forceinline__ void load_baseline(const S1Args& a, int ih, bool raw,
   b.cls = kClsHid;
 }
 
+// Half-turn dithering (FP32 modes): MUFU sin/cos carry a small mean error over
+// the angle range, which a sum over ~1e6 pixels would add coherently.  Odd
+// pixels are evaluated half a turn further on and their partial sums are
+// subtracted (exp(i(t + pi)) = -exp(i t)), so the two parities' mean errors
+// cancel.  PAR = 1 selects the shifted evaluation.
 template <int MODE>
+__device__ constexpr bool pixel_dither() {
+  return MODE == VB_PREC_FP32_FP64PH || MODE == VB_PREC_FP32_DSPH;
+}
+
+template <int MODE, int PAR>
 __device__ __forceinline__ void phase_sincos(const Baseline& b, const double2 lm, const double nd,
                                              const float4 f, const float nm1, float& s, float& c,
                                              double& sd, double& cd, bool raw) {
   if constexpr (MODE == VB_PREC_FP32_FP64PH) {
     double t = fma(b.U, lm.x, fma(b.V, lm.y, fma(b.W, nd, b.C)));
     unsigned lo = (unsigned)__double2loint(t);
+    if constexpr (PAR) lo ^= 1u << (kFracShift + 22);   // + 1/2 turn (top fraction bit)
     unsigned kb = ((lo >> kFracShift) & 0x7FFFFFu) | 0x4B000000u;
     float ang = __fmaf_rn(__uint_as_float(kb), kAngScale, -kTwoPiF);
     __sincosf(ang, &s, &c);
@@ -149,6 +160,10 @@ __device__ __forceinline__ void phase_sincos(const Baseline& b, const double2 lm
     float efr = __fadd_rn(__fadd_rn(e1, e2), e3);
     float t = __fadd_rn(sfr, efr);
     t = __fsub_rn(t, rint_magic(t));
+    if constexpr (PAR) {
+      t = __fadd_rn(t, 0.5f);
+      t = __fsub_rn(t, rint_magic(t));
+    }
     __sincosf(__fmul_rn(t, kTwoPiF), &s, &c);
   } else if constexpr (MODE == VB_PREC_REF32) {
     float ang = raw ? fmaf(b.kw, nm1, fmaf(b.kv, f.y, b.ku * f.x))
@@ -266,8 +281,9 @@ __global__ void __launch_bounds__(S1_THREADS, 2) k_stage1(const S1Args a) {
 
         // one pixel: MASKED selects the per-pixel occlusion test for mixed
         // baselines (visible ones included unconditionally, hidden excluded)
-        auto pixel = [&](const int j, float (&aR)[BPT], float (&aI)[BPT], auto masked_tag) {
+        auto pixel = [&](const int j, float (&aR)[BPT], float (&aI)[BPT], auto masked_tag, auto par_tag) {
           constexpr bool MASKED = decltype(masked_tag)::value;
+          constexpr int PAR = decltype(par_tag)::value;
           const double2 lm = s_lm[j];
           const float4 nb = s_nb[j];
           const double nd = __hiloint2double(__float_as_int(nb.y), __float_as_int(nb.x));
@@ -287,7 +303,7 @@ __global__ void __launch_bounds__(S1_THREADS, 2) k_stage1(const S1Args a) {
             }
             float sn, cs;
             double sd, cd;
-            phase_sincos<MODE>(b, lm, nd, f, nb.w, sn, cs, sd, cd, raw);
+            phase_sincos<MODE, PAR>(b, lm, nd, f, nb.w, sn, cs, sd, cd, raw);
             if constexpr (kDoubleAcc) {
               const double Bw = inc ? (double)Bp : 0.0;
               dR[k] = fma(Bw, cd, dR[k]);
@@ -301,21 +317,25 @@ __global__ void __launch_bounds__(S1_THREADS, 2) k_stage1(const S1Args a) {
         };
         using Unmasked = std::false_type;
         using Masked = std::true_type;
+        using Even = std::integral_constant<int, 0>;
+        using Odd = std::integral_constant<int, pixel_dither<MODE>() ? 1 : 0>;
 
         int j = 0;
         if (!warp_mix) {
           for (; j + 1 < ns; j += 2) {
-            pixel(j, pR0, pI0, Unmasked{});
-            pixel(j + 1, pR1, pI1, Unmasked{});
+            pixel(j, pR0, pI0, Unmasked{}, Even{});
+            pixel(j + 1, pR1, pI1, Unmasked{}, Odd{});
           }
-          if (j < ns) pixel(j, pR0, pI0, Unmasked{});
+          if (j < ns) pixel(j, pR0, pI0, Unmasked{}, Even{});
         } else {
           for (; j + 1 < ns; j += 2) {
-            pixel(j, pR0, pI0, Masked{});
-            pixel(j + 1, pR1, pI1, Masked{});
+            pixel(j, pR0, pI0, Masked{}, Even{});
+            pixel(j + 1, pR1, pI1, Masked{}, Odd{});
           }
-          if (j < ns) pixel(j, pR0, pI0, Masked{});
+          if (j < ns) pixel(j, pR0, pI0, Masked{}, Even{});
         }
+        // the odd-pixel sums were taken half a turn on: subtract them
+        constexpr float kOddSign = pixel_dither<MODE>() ? -1.0f : 1.0f;
 
         // fold the staged-tile partials into the running totals
 #pragma unroll
@@ -326,8 +346,8 @@ __global__ void __launch_bounds__(S1_THREADS, 2) k_stage1(const S1Args a) {
             accI[k] += dI[k];
           } else if constexpr (MODE == VB_PREC_FP32_DSPH) {
             // Kahan summation in FP32 across staged tiles
-            float xr = __fadd_rn(pR0[k], pR1[k]);
-            float xi = __fadd_rn(pI0[k], pI1[k]);
+            float xr = __fmaf_rn(kOddSign, pR1[k], pR0[k]);
+            float xi = __fmaf_rn(kOddSign, pI1[k], pI0[k]);
             float sr = (float)accR[k], si = (float)accI[k];
             float yr = __fsub_rn(xr, kcR[k]);
             float tr = __fadd_rn(sr, yr);
@@ -338,8 +358,8 @@ __global__ void __launch_bounds__(S1_THREADS, 2) k_stage1(const S1Args a) {
             accR[k] = tr;
             accI[k] = ti;
           } else {
-            accR[k] += (double)pR0[k] + (double)pR1[k];
-            accI[k] += (double)pI0[k] + (double)pI1[k];
+            accR[k] += (double)pR0[k] + (double)kOddSign * (double)pR1[k];
+            accI[k] += (double)pI0[k] + (double)kOddSign * (double)pI1[k];
           }
         }
       }

@@ -19,6 +19,7 @@
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
 #include <cmath>
+#include <type_traits>
 
 #include "vb_common.cuh"
 #include "vb_geom.cuh"
@@ -27,7 +28,7 @@
 namespace vb {
 
 constexpr int S2_THREADS = 256;
-constexpr int S2_STAGE = 128;            // group records staged per step
+constexpr int S2_STAGE = S2_THREADS;     // group records staged per step (one per thread)
 constexpr double kMagic2 = 12582912.0;   // 1.5 * 2^23, see stage 1
 constexpr double kHalfLsb2 = 5.9604644775390625e-8;
 constexpr int kFracShift2 = 6;
@@ -346,16 +347,136 @@ __device__ __forceinline__ void recon_phase(const GroupRec& g, double ld, double
   }
 }
 
-// occ_mode 2 (representative) and blockage=0 (group averages) paths.
+// Per-group data read by the term loop of k_recon_rec, 32 bytes in every mode.
+// vx, nvy = Re V, -Im V of the group's visibility (times -1 in the odd slots
+// of a dithered mode, see rec_term).
 template <int MODE>
+struct TermRec {          // FP64, FP32 with FP64 phase: t = a l + b m + c n
+  double a, b, c;
+  float vx, nvy;
+};
+template <>
+struct TermRec<VB_PREC_FP32_DSPH> {   // double-single phase: a, b and c = chi + clo as floats
+  float af, bf, chi, clo, vx, nvy, pad0, pad1;
+};
+template <>
+struct TermRec<VB_PREC_REF32> {       // upstream FP32 arithmetic: (ugu, vgu, fa, fb)
+  float ugu, vgu, fa, fb, vx, nvy, pad0, pad1;
+};
+struct OccRec {           // occlusion data of a mixed group
+  float4 p1, p2;
+  float cp1, cp2;
+};
+
+// Half-turn dithering.  MUFU sin/cos carry a small mean error over the angle
+// range, and a term-by-term sum of ~1e4-1e6 terms would add it coherently.  In
+// the FP32 modes the odd slot of every pair of staged groups is evaluated half
+// a turn further on (exp(i(t + pi)) = -exp(i t)) with its visibility negated,
+// so the products are unchanged and the two slots' mean errors cancel.
+template <int MODE>
+__device__ constexpr bool rec_dither() {
+  return MODE == VB_PREC_FP32_FP64PH || MODE == VB_PREC_FP32_DSPH;
+}
+
+template <int MODE>
+__device__ __forceinline__ TermRec<MODE> make_term(const GroupRec& g, bool odd) {
+  TermRec<MODE> t;
+  const float sg = (rec_dither<MODE>() && odd) ? -1.0f : 1.0f;
+  if constexpr (MODE == VB_PREC_FP32_DSPH) {
+    t.af = (float)g.a; t.bf = (float)g.b; t.chi = g.chi; t.clo = g.clo; t.pad0 = t.pad1 = 0.f;
+  } else if constexpr (MODE == VB_PREC_REF32) {
+    t.ugu = (float)g.a; t.vgu = (float)g.b; t.fa = g.fa; t.fb = g.fb; t.pad0 = t.pad1 = 0.f;
+  } else {
+    t.a = g.a; t.b = g.b; t.c = g.c;
+  }
+  t.vx = sg * g.vx;
+  t.nvy = -(sg * g.vy);
+  return t;
+}
+
+template <int MODE>
+__device__ __forceinline__ TermRec<MODE> zero_term() {
+  return TermRec<MODE>{};
+}
+
+// Pixel coordinates of one reconstruction pixel.
+struct RecPix {
+  double ld, md, nd;
+  float lf, mf, nf;
+};
+
+// Re(V exp(+2 pi i t)) of one (group, pixel) term accumulated into acc.
+// PAR = 1 adds the half turn of the odd dither slot.
+template <int MODE, int PAR, class Acc>
+__device__ __forceinline__ void rec_term(const TermRec<MODE>& r, const RecPix& p, Acc& acc) {
+  if constexpr (MODE == VB_PREC_FP32_FP64PH) {
+    constexpr double K = kMagic2 + kHalfLsb2 + (PAR ? 0.5 : 0.0);
+    const double t = fma(r.a, p.ld, fma(r.b, p.md, fma(r.c, p.nd, K)));
+    const unsigned lo = (unsigned)__double2loint(t);
+    const unsigned kb = ((lo >> kFracShift2) & 0x7FFFFFu) | 0x4B000000u;
+    const float ang = __fmaf_rn(__uint_as_float(kb), kAngScale2, -kTwoPiF2);
+    float s, c;
+    __sincosf(ang, &s, &c);
+    acc = fmaf(r.vx, c, acc);
+    acc = fmaf(r.nvy, s, acc);
+  } else if constexpr (MODE == VB_PREC_FP32_DSPH) {
+    auto rn = [](float x) { return __fsub_rn(__fadd_rn(x, 12582912.0f), 12582912.0f); };
+    const float p1 = __fmul_rn(r.af, p.lf), e1 = __fmaf_rn(r.af, p.lf, -p1);
+    const float p2 = __fmul_rn(r.bf, p.mf), e2 = __fmaf_rn(r.bf, p.mf, -p2);
+    const float p3 = __fmul_rn(r.chi, p.nf), e3 = __fmaf_rn(r.chi, p.nf, -p3);
+    const float fr = __fadd_rn(__fadd_rn(__fsub_rn(p1, rn(p1)), __fsub_rn(p2, rn(p2))), __fsub_rn(p3, rn(p3)));
+    const float er = __fadd_rn(__fadd_rn(e1, e2), __fmaf_rn(r.clo, p.nf, e3));
+    float t = __fadd_rn(fr, er);
+    t = __fsub_rn(t, rn(t));
+    if constexpr (PAR) {
+      t = __fadd_rn(t, 0.5f);
+      t = __fsub_rn(t, rn(t));
+    }
+    float s, c;
+    __sincosf(__fmul_rn(t, kTwoPiF2), &s, &c);
+    acc = fmaf(r.vx, c, acc);
+    acc = fmaf(r.nvy, s, acc);
+  } else if constexpr (MODE == VB_PREC_REF32) {
+    // upstream: phase = 2 pi (ugu (l + fa n) + vgu (m + fb n)) in FP32
+    // (viss_recon_kernel.cuh:620-626, ..._vissfast.cuh:1270-1276)
+    const float TWO_PI = 6.2831853071795864769f;
+    const float lp = p.lf + r.fa * p.nf;
+    const float mp = p.mf + r.fb * p.nf;
+    const float phase = TWO_PI * (r.ugu * lp + r.vgu * mp);
+    float s, c;
+    __sincosf(phase, &s, &c);
+    acc += fmaf(r.vx, c, r.nvy * s);
+  } else {
+    const double t = fma(r.a, p.ld, fma(r.b, p.md, r.c * p.nd));
+    double s, c;
+    sincospi(2.0 * t, &s, &c);
+    acc = fma((double)r.vx, c, acc);
+    acc = fma((double)r.nvy, s, acc);
+  }
+}
+
+// occ_mode 2 (representative) and blockage=0 (group averages) paths.
+//
+// Work item = (pixel block of PPT * 256 pixels, chunk of groups).  Each thread
+// owns PPT pixels.  Per stage of up to 256 groups the CTA classifies every
+// group against the block (hidden / visible / mixed; exact cones with
+// VB_CULL_EXACT, otherwise mixed) and compacts the visible and the mixed ones
+// into two lists in shared memory; the term loop then runs without branches
+// over the visible list and with the per-pixel occlusion test over the mixed
+// list, two groups (the dither pair) by PPT pixels per step.
+template <int MODE, int PPT>
 __global__ void __launch_bounds__(S2_THREADS, 2) k_recon_rec(const ReconArgs a) {
-  __shared__ GroupRec s_rec[S2_STAGE];
-  __shared__ int s_cls[S2_STAGE];
+  constexpr int NW = S2_THREADS / 32;
+  __shared__ TermRec<MODE> s_vis[S2_STAGE + 1];
+  __shared__ TermRec<MODE> s_mix[S2_STAGE + 1];
+  __shared__ OccRec s_occ[S2_STAGE + 1];
+  __shared__ int s_wv[NW], s_wm[NW];
   __shared__ int s_item;
-  __shared__ unsigned long long s_cnt[4];
   __shared__ ExactCone s_cone;
   constexpr bool kDouble = (MODE == VB_PREC_FP64);
-  if (threadIdx.x < 4) s_cnt[threadIdx.x] = 0ull;
+  using Acc = typename std::conditional<kDouble, double, float>::type;
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
   const int ng = *a.ngroups;
   const int nchunk = (ng + a.gchunk - 1) / a.gchunk;
   const int n_items = nchunk * a.nblocks;
@@ -369,88 +490,147 @@ __global__ void __launch_bounds__(S2_THREADS, 2) k_recon_rec(const ReconArgs a) 
     if (item >= n_items) break;
     const int gc = item / a.nblocks;
     const int blk = item - gc * a.nblocks;
-    const int64_t pix = (int64_t)blk * a.block_pix + threadIdx.x;
-    const bool active = pix < a.npix;
     if (a.cull == VB_CULL_EXACT && threadIdx.x == 0) s_cone = a.cones[blk];
-    float lf = 0.f, mf = 0.f, nf = 0.f;
-    double ld = 0.0, md = 0.0, nd = 0.0;
-    if (active) {
-      const float4 f = a.f4[pix];
-      lf = f.x; mf = f.y; nf = f.z;
-      const double2 lm = a.lm[pix];
-      const float4 nbr = a.nb[pix];
-      ld = lm.x; md = lm.y;
-      nd = __hiloint2double(__float_as_int(nbr.y), __float_as_int(nbr.x));
+    const int64_t pix0 = (int64_t)blk * a.block_pix;
+    const int npx_blk = (int)min((int64_t)a.block_pix, a.npix - pix0);
+
+    RecPix px[PPT];
+    bool act[PPT];
+#pragma unroll
+    for (int q = 0; q < PPT; ++q) {
+      const int64_t pix = pix0 + q * S2_THREADS + threadIdx.x;
+      act[q] = pix < a.npix;
+      px[q] = RecPix{0.0, 0.0, 0.0, 0.f, 0.f, 0.f};
+      if (act[q]) {
+        const float4 f = a.f4[pix];
+        const double2 lm = a.lm[pix];
+        const float4 nbr = a.nb[pix];
+        px[q] = RecPix{lm.x, lm.y, __hiloint2double(__float_as_int(nbr.y), __float_as_int(nbr.x)), f.x, f.y, f.z};
+      }
     }
-    const int npx_blk = (int)min((int64_t)a.block_pix, a.npix - (int64_t)blk * a.block_pix);
-    double totC = 0.0;
-    float kc = 0.f;
-    unsigned totW = 0;
+    double totC[PPT];
+    float kc[PPT];
+    unsigned totW[PPT];
+#pragma unroll
+    for (int q = 0; q < PPT; ++q) { totC[q] = 0.0; kc[q] = 0.f; totW[q] = 0u; }
+
     const int g_begin = gc * a.gchunk;
     const int g_end = min(ng, g_begin + a.gchunk);
     for (int gs = g_begin; gs < g_end; gs += S2_STAGE) {
       const int nst = min(S2_STAGE, g_end - gs);
-      __syncthreads();
-      for (int j = threadIdx.x; j < nst; j += S2_THREADS) {
-        GroupRec r = a.rec[gs + j];
-        int cls = 2;
-        if (r.flags & 1) cls = 0;
+      __syncthreads();   // previous stage's lists fully read; s_cone visible
+      // --- classify this stage's groups and compact them ---------------------
+      int cls = 0;
+      GroupRec r;
+      if ((int)threadIdx.x < nst) {
+        r = a.rec[gs + threadIdx.x];
+        if (r.flags & 3) cls = 0;              // key 0, or non-finite V: neither summed nor counted
         else if (!a.blockage) cls = 1;
         else if (a.cull == VB_CULL_EXACT) {
-          int e1 = exact_class(s_cone, r.p1.x, r.p1.y, r.p1.z, r.p1.w, r.cp1);
-          int e2 = exact_class(s_cone, r.p2.x, r.p2.y, r.p2.z, r.p2.w, r.cp2);
+          const int e1 = exact_class(s_cone, r.p1.x, r.p1.y, r.p1.z, r.p1.w, r.cp1);
+          const int e2 = exact_class(s_cone, r.p2.x, r.p2.y, r.p2.z, r.p2.w, r.cp2);
           cls = (e1 < 0 || e2 < 0) ? 0 : ((e1 > 0 && e2 > 0) ? 1 : 2);
+        } else {
+          cls = 2;
         }
-        s_rec[j] = r;
-        s_cls[j] = cls;
+      }
+      const unsigned bv = __ballot_sync(0xffffffffu, cls == 1);
+      const unsigned bm = __ballot_sync(0xffffffffu, cls == 2);
+      if (lane == 0) { s_wv[warp] = __popc(bv); s_wm[warp] = __popc(bm); }
+      __syncthreads();
+      int ov = 0, om = 0, nv = 0, nm = 0;
+#pragma unroll
+      for (int w = 0; w < NW; ++w) {
+        const int cv = s_wv[w], cm = s_wm[w];
+        if (w < warp) { ov += cv; om += cm; }
+        nv += cv;
+        nm += cm;
+      }
+      const unsigned below = (1u << lane) - 1u;
+      if (cls == 1) {
+        const int k = ov + __popc(bv & below);
+        s_vis[k] = make_term<MODE>(r, k & 1);
+      } else if (cls == 2) {
+        const int k = om + __popc(bm & below);
+        s_mix[k] = make_term<MODE>(r, k & 1);
+        s_occ[k] = OccRec{r.p1, r.p2, r.cp1, r.cp2};
+      }
+      if (threadIdx.x == 0) {
+        // pad odd lists with a record that adds nothing (and fails the test)
+        if (nv & 1) s_vis[nv] = zero_term<MODE>();
+        if (nm & 1) {
+          s_mix[nm] = zero_term<MODE>();
+          s_occ[nm] = OccRec{make_float4(0.f, 0.f, 0.f, 0.f), make_float4(0.f, 0.f, 0.f, 0.f), INFINITY, INFINITY};
+        }
+        c_fast += (unsigned long long)nv * npx_blk;
+        c_mask += (unsigned long long)nm * npx_blk;
+        c_hid += (unsigned long long)(nst - nv - nm) * npx_blk;
+        c_all += (unsigned long long)nst * npx_blk;
       }
       __syncthreads();
-      float accf = 0.f;
-      double accd = 0.0;
-      for (int j = 0; j < nst; ++j) {
-        const int cls = s_cls[j];
-        if (cls == 0) {
-          if (threadIdx.x == 0) c_hid += npx_blk;
-          continue;
+
+      // --- visible groups: no test ---------------------------------------------
+      Acc e[PPT], o[PPT];
+#pragma unroll
+      for (int q = 0; q < PPT; ++q) { e[q] = Acc(0); o[q] = Acc(0); }
+      for (int k = 0; k < nv; k += 2) {
+        const TermRec<MODE> r0 = s_vis[k];
+        const TermRec<MODE> r1 = s_vis[k + 1];
+#pragma unroll
+        for (int q = 0; q < PPT; ++q) {
+          rec_term<MODE, 0>(r0, px[q], e[q]);
+          rec_term<MODE, 1>(r1, px[q], o[q]);
         }
-        const GroupRec& r = s_rec[j];
-        bool inc = active;
-        if (cls == 2) {
-          const float o1 = occ_dot(lf, mf, nf, r.p1.x, r.p1.y, r.p1.z, r.p1.w);
-          const float o2 = occ_dot(lf, mf, nf, r.p2.x, r.p2.y, r.p2.z, r.p2.w);
-          inc = inc && (o1 >= r.cp1 && o2 >= r.cp2);
-          if (threadIdx.x == 0) c_mask += npx_blk;
-        } else if (threadIdx.x == 0) {
-          c_fast += npx_blk;
-        }
-        if (r.flags & 2) inc = false;
-        float s, c;
-        double sd, cd;
-        recon_phase<MODE>(r, ld, md, nd, lf, mf, nf, s, c, sd, cd);
-        if constexpr (kDouble) {
-          if (inc) accd += (double)r.vx * cd - (double)r.vy * sd;
-        } else {
-          const float t = fmaf(r.vx, c, -r.vy * s);
-          accf += inc ? t : 0.0f;
-        }
-        if (a.blockage) totW += inc ? 1u : 0u;
       }
-      if constexpr (kDouble) {
-        totC += accd;
-      } else if constexpr (MODE == VB_PREC_FP32_DSPH) {
-        float sr = (float)totC;
-        float y = __fsub_rn(accf, kc);
-        float t = __fadd_rn(sr, y);
-        kc = __fsub_rn(__fsub_rn(t, sr), y);
-        totC = t;
-      } else {
-        totC += (double)accf;
+      if (a.blockage) {
+#pragma unroll
+        for (int q = 0; q < PPT; ++q) totW[q] += (unsigned)nv;
+      }
+      // --- mixed groups: per-pixel occlusion test ------------------------------
+      for (int k = 0; k < nm; k += 2) {
+        const TermRec<MODE> r0 = s_mix[k];
+        const TermRec<MODE> r1 = s_mix[k + 1];
+        const OccRec c0 = s_occ[k];
+        const OccRec c1 = s_occ[k + 1];
+#pragma unroll
+        for (int q = 0; q < PPT; ++q) {
+          const RecPix& p = px[q];
+          const bool in0 = occ_dot(p.lf, p.mf, p.nf, c0.p1.x, c0.p1.y, c0.p1.z, c0.p1.w) >= c0.cp1 &&
+                           occ_dot(p.lf, p.mf, p.nf, c0.p2.x, c0.p2.y, c0.p2.z, c0.p2.w) >= c0.cp2;
+          const bool in1 = occ_dot(p.lf, p.mf, p.nf, c1.p1.x, c1.p1.y, c1.p1.z, c1.p1.w) >= c1.cp1 &&
+                           occ_dot(p.lf, p.mf, p.nf, c1.p2.x, c1.p2.y, c1.p2.z, c1.p2.w) >= c1.cp2;
+          Acc t0 = Acc(0), t1 = Acc(0);
+          rec_term<MODE, 0>(r0, p, t0);
+          rec_term<MODE, 1>(r1, p, t1);
+          e[q] += in0 ? t0 : Acc(0);
+          o[q] += in1 ? t1 : Acc(0);
+          totW[q] += (in0 ? 1u : 0u) + (in1 ? 1u : 0u);
+        }
+      }
+      // --- fold the stage sums into the totals -------------------------------
+#pragma unroll
+      for (int q = 0; q < PPT; ++q) {
+        if constexpr (kDouble) {
+          totC[q] += e[q] + o[q];
+        } else if constexpr (MODE == VB_PREC_FP32_DSPH) {
+          const float x = __fadd_rn(e[q], o[q]);
+          const float sr = (float)totC[q];
+          const float y = __fsub_rn(x, kc[q]);
+          const float t = __fadd_rn(sr, y);
+          kc[q] = __fsub_rn(__fsub_rn(t, sr), y);
+          totC[q] = t;
+        } else {
+          totC[q] += (double)e[q] + (double)o[q];
+        }
       }
     }
-    if (threadIdx.x == 0) c_all += (int64_t)npx_blk * (g_end - g_begin);
-    if (active) {
-      a.Cpart[(int64_t)gc * a.npix + pix] = totC;
-      a.Wpart[(int64_t)gc * a.npix + pix] = totW;
+#pragma unroll
+    for (int q = 0; q < PPT; ++q) {
+      if (act[q]) {
+        const int64_t pix = pix0 + q * S2_THREADS + threadIdx.x;
+        a.Cpart[(int64_t)gc * a.npix + pix] = totC[q];
+        a.Wpart[(int64_t)gc * a.npix + pix] = totW[q];
+      }
     }
   }
   if (a.counters && threadIdx.x == 0) {
@@ -600,14 +780,19 @@ int stage2_plan(int n_half_total, int nseg, int64_t npix, const vb_stage2_opts* 
   q.precision = o->precision;
   q.cull = (o->cull == VB_CULL_EXACT && q.blockage && q.occ_mode == 2) ? VB_CULL_EXACT : VB_CULL_NONE;
   q.grid_res = o->grid_res;
-  q.ppt = 1;
+  // pixels per thread of the representative / average path (the member path
+  // keeps one): 2 by default, 1, 2 or 4 on request
+  if (o->ppt != 0 && o->ppt != 1 && o->ppt != 2 && o->ppt != 4)
+    return fail(VB_ERR_INVALID, "stage 2: ppt=%d (0, 1, 2 or 4)", o->ppt);
+  const bool members = q.blockage && q.occ_mode != 2;
+  q.ppt = members ? 1 : (o->ppt == 0 ? 2 : o->ppt);
   q.bl_max = o->bl_max;
   q.lambda = o->lambda;
   q.n_half_total = n_half_total;
   q.n_keyed_total = q.mirror ? n_half_total : 2 * n_half_total;
   q.nseg = nseg;
   q.npix = npix;
-  q.block_pix = S2_THREADS;
+  q.block_pix = S2_THREADS * q.ppt;
   q.nblocks = (int)ceil_div(npix, q.block_pix);
   const int capacity = sm_count() * 2;
   const int64_t want_items = (int64_t)capacity * 8;
@@ -692,20 +877,24 @@ size_t stage2_workspace(const Stage2Plan& p, void* ws, size_t cap, void** slices
   return r;
 }
 
-template <int MODE>
-static int launch_recon(const ReconArgs& a, bool members, cudaStream_t s) {
+template <class K>
+static int launch_persistent(K kern, const ReconArgs& a, cudaStream_t s) {
   int occ = 0;
-  if (members) {
-    VB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_recon_members<MODE>, S2_THREADS, 0));
-  } else {
-    VB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_recon_rec<MODE>, S2_THREADS, 0));
-  }
+  VB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, S2_THREADS, 0));
   if (occ < 1) occ = 1;
-  int grid = sm_count() * occ;
-  if (members) k_recon_members<MODE><<<grid, S2_THREADS, 0, s>>>(a);
-  else k_recon_rec<MODE><<<grid, S2_THREADS, 0, s>>>(a);
+  kern<<<sm_count() * occ, S2_THREADS, 0, s>>>(a);
   VB_LAUNCH_CHECK();
   return VB_OK;
+}
+
+template <int MODE>
+static int launch_recon(const ReconArgs& a, bool members, int ppt, cudaStream_t s) {
+  if (members) return launch_persistent(k_recon_members<MODE>, a, s);
+  switch (ppt) {
+    case 1: return launch_persistent(k_recon_rec<MODE, 1>, a, s);
+    case 4: return launch_persistent(k_recon_rec<MODE, 4>, a, s);
+    default: return launch_persistent(k_recon_rec<MODE, 2>, a, s);
+  }
 }
 
 __global__ void k_expand_half(const float* __restrict__ Vh, int n_half, int nbl, float* __restrict__ Vf) {
@@ -803,10 +992,10 @@ int stage2_run(const vb_sky* sky, const vb_baselines* bl, const float* V_half, i
     VB_CUDA(cudaMemsetAsync(x.queue, 0, sizeof(int), st));
     if (kbeg) VB_CUDA(record_event(kbeg, st));
     switch (p.precision) {
-      case VB_PREC_REF32: VB_TRY(launch_recon<VB_PREC_REF32>(ra, members, st)); break;
-      case VB_PREC_FP64: VB_TRY(launch_recon<VB_PREC_FP64>(ra, members, st)); break;
-      case VB_PREC_FP32_FP64PH: VB_TRY(launch_recon<VB_PREC_FP32_FP64PH>(ra, members, st)); break;
-      default: VB_TRY(launch_recon<VB_PREC_FP32_DSPH>(ra, members, st)); break;
+      case VB_PREC_REF32: VB_TRY(launch_recon<VB_PREC_REF32>(ra, members, p.ppt, st)); break;
+      case VB_PREC_FP64: VB_TRY(launch_recon<VB_PREC_FP64>(ra, members, p.ppt, st)); break;
+      case VB_PREC_FP32_FP64PH: VB_TRY(launch_recon<VB_PREC_FP32_FP64PH>(ra, members, p.ppt, st)); break;
+      default: VB_TRY(launch_recon<VB_PREC_FP32_DSPH>(ra, members, p.ppt, st)); break;
     }
     if (kend) VB_CUDA(record_event(kend, st));
   } else if (kbeg) {
