@@ -62,6 +62,9 @@ def parse() -> argparse.Namespace:
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 GPU comparison run")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--shape", default="auto",
+                    help="kernel shapes: 'auto' (autotuned before the warm-up, untimed), 'default' (built-in), "
+                         "or 'bpt,stage_pix,ctas_per_sm,items_per_cta/ppt,items_per_cta' for stage 1 / stage 2")
     return ap.parse_args()
 
 
@@ -295,9 +298,20 @@ def main() -> None:
     vb.check(L.vb_measure_peaks(C.byref(sfu), C.byref(f32), C.byref(f64), C.byref(clk)))
 
     B = vb.synthetic_sky(256, seed=1)
-    p = vb.Pipeline(vb.run_config(**workload_kwargs()))
+    kw = workload_kwargs()
+    if args.shape not in ("auto", "default"):
+        s1, s2 = args.shape.split("/")
+        b, sp, ct, it = (int(x) for x in s1.split(","))
+        pp, it2 = (int(x) for x in s2.split(","))
+        kw.update(stage1_bpt=b, stage1_stage_pix=sp, stage1_ctas_per_sm=ct, stage1_items_per_cta=it,
+                  stage2_ppt=pp, stage2_items_per_cta=it2)
+    p = vb.Pipeline(vb.run_config(**kw))
     p.set_sky(B)
     p.make_baselines()
+    tune = p.autotune(reps=2) if args.shape == "auto" else None
+    shape = (f"{tune['stage1_bpt']},{tune['stage1_stage_pix']},{tune['stage1_ctas_per_sm']},"
+             f"{tune['stage1_items_per_cta']}/{tune['stage2_ppt']},{tune['stage2_items_per_cta']}"
+             if tune else args.shape)
     for _ in range(max(3, args.warmup)):
         p.run()
     flush = vb.DeviceBuffer(512 << 20)
@@ -361,6 +375,7 @@ def main() -> None:
         q = vb.Pipeline(vb.run_config(**workload_kwargs("fp64")))
         q.set_sky(B)
         q.make_baselines()
+        tune64 = q.autotune(reps=1) if args.shape == "auto" else None   # the FP64 build gets its own best shapes
         q.run()
         tq = []
         for _ in range(2):
@@ -374,7 +389,7 @@ def main() -> None:
         ec = rel_errs(Cmixed, C64)
         t64 = dist.max(min(tq))
         fp64 = {"value": ws * terms_step / (t64 * 1e-3) / 1e9, "ms_per_step": t64,
-                "speedup_mixed_vs_fp64": t64 / ms_per_step,
+                "speedup_mixed_vs_fp64": t64 / ms_per_step, "autotune": tune64,
                 "error_vs_fp64": {"V_max": ev[0], "V_rms": ev[1], "C_max": ec[0], "C_rms": ec[1]}}
     dist.barrier()
 
@@ -409,6 +424,7 @@ def main() -> None:
            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f32+f64phase", "data": "synthetic",
            "config": dict(WORKLOAD, parallelism=f"replicas{ws}", l2="flushed between steps (512 MiB write)",
+                          kernel_shape=shape, autotune=tune,
                           terms_per_step=terms_step, stage1_terms=r["stage1_terms"], stage2_terms=r["stage2_terms"],
                           groups=r["groups_total"]),
            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,

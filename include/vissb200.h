@@ -186,6 +186,8 @@ typedef struct {
   int stage_pix;        /* pixels staged in shared memory per step (0 = auto) */
   int chunk_pix;        /* pixels per work item (0 = auto) */
   int exact_tile_pix;   /* tile of the VB_CULL_EXACT cones (0 = auto) */
+  int ctas_per_sm;      /* resident CTAs per SM the kernel is built for: 2, or 3 with bpt <= 2 (0 = 2) */
+  int items_per_cta;    /* work-queue items per resident CTA when chunk_pix = 0 (0 = auto) */
 } vb_stage1_opts;
 
 size_t vb_stage1_workspace_bytes(const vb_sky* sky, const vb_baselines* bl,
@@ -262,6 +264,7 @@ typedef struct {
   float bl_max;         /* metres */
   float lambda;         /* metres */
   int ppt;              /* pixels per thread of the occ_mode=2 / blockage=0 path: 1, 2 or 4 (0 = 2) */
+  int items_per_cta;    /* work-queue items (pixel block x group chunk) per resident CTA (0 = auto) */
 } vb_stage2_opts;
 
 typedef struct {       /* per-segment plane-fit and grid numbers, device or host copy */
@@ -332,6 +335,11 @@ typedef struct {
   uint64_t seg_seed;
   int      stage2_cull;    /* 2: exact pixel-block culling in stage 2, 0: off */
   int      stage2_ppt;     /* stage-2 pixels per thread (vb_stage2_opts.ppt; 0 = auto) */
+  int      stage2_items_per_cta;  /* vb_stage2_opts.items_per_cta */
+  int      stage1_bpt;            /* vb_stage1_opts.bpt */
+  int      stage1_stage_pix;      /* vb_stage1_opts.stage_pix */
+  int      stage1_ctas_per_sm;    /* vb_stage1_opts.ctas_per_sm */
+  int      stage1_items_per_cta;  /* vb_stage1_opts.items_per_cta */
   int      use_graph;      /* 1: capture stages in one CUDA graph */
   int      device;         /* CUDA device ordinal */
 } vb_run_config;
@@ -393,6 +401,30 @@ int vb_pipeline_info(vb_pipeline* p, int64_t* npix, int* nseg, int* n_half_total
 int vb_pipeline_seg_plan(vb_pipeline* p, int* seg_t0, int* seg_tlen);   /* host arrays of nseg */
 int vb_pipeline_seg_params(vb_pipeline* p, vb_seg_params* host_out);     /* host array of nseg; syncs */
 int vb_pipeline_destroy(vb_pipeline* p);
+
+/* Autotuner (no upstream counterpart: upstream fixes 256-thread blocks and one
+ * block per 256 baselines or pixels).  Times the stage-1 kernel over baselines
+ * per thread x staged pixels x resident CTAs per SM x work-queue granularity,
+ * then the stage-2 kernel over pixels per thread x granularity, on this
+ * pipeline's own resident inputs (sky and baselines must be set), keeps the
+ * fastest shape of each stage in the pipeline's config (the next run
+ * re-captures its graph) and reports it.  reps: timed runs per candidate
+ * (min taken; 0 = 2).  The pipeline's workspaces grow when a candidate needs
+ * more; nothing else is allocated. */
+typedef struct {
+  int    stage1_bpt, stage1_stage_pix, stage1_ctas_per_sm, stage1_items_per_cta;
+  int    stage2_ppt, stage2_items_per_cta;
+  double stage1_ms, stage2_ms;                 /* best kernel times */
+  double stage1_default_ms, stage2_default_ms; /* the untuned (auto) shapes */
+  int    candidates;                           /* shapes timed */
+} vb_tune_report;
+int vb_pipeline_autotune(vb_pipeline* p, int reps, vb_tune_report* out);
+
+/* sizeof() of a public struct by its type name ("vb_sky", "vb_baselines",
+ * "vb_stage1_opts", "vb_stage2_opts", "vb_seg_params", "vb_orbit_params",
+ * "vb_run_config", "vb_report", "vb_tune_report"); 0 for an unknown name.
+ * Lets FFI bindings check their struct layouts. */
+size_t vb_abi_sizeof(const char* type_name);
 
 /* ------------------------------------------------------------------------ */
 /* measurement helpers                                                        */

@@ -65,3 +65,18 @@ def test_host_only_entry_points(vb):
     B = np.empty(12 * 4 * 4, np.float32)
     assert lib.vb_make_synthetic_sky(4, 3, 2, 10.0, B.ctypes.data) == 0
     assert B.min() >= 0 and B.max() >= 10.0
+
+
+def test_struct_layouts_match_bindings(vb):
+    """Every public struct has the size the ctypes binding assumes (a layout
+    slip would pass garbage through the ABI)."""
+    import ctypes as C
+    from viss_optimize_ws_b200._lib import ABI_STRUCTS
+    lib = vb.lib()
+    for name, cls in ABI_STRUCTS.items():
+        assert lib.vb_abi_sizeof(name.encode()) == C.sizeof(cls), name
+    assert lib.vb_abi_sizeof(b"no_such_struct") == 0
+    # every typedef'd struct of the header is covered
+    text = (ROOT / "include" / "vissb200.h").read_text()
+    declared = set(re.findall(r"}\s*(vb_[a-z0-9_]+)\s*;", text))
+    assert declared == set(ABI_STRUCTS), declared ^ set(ABI_STRUCTS)

@@ -91,3 +91,30 @@ def test_dropin_error_paths(tmp_path):
     r = run(exe, ["--btag=1M", "--nside=8", f"--sky_dir={tmp_path}/s", "--B_mode=bin", f"--out_dir={tmp_path}/o/"],
             tmp_path)
     assert r.returncode == 1 and "ERROR reading B" in r.stderr
+
+
+def test_parameter_scripts_and_autotune(gpu, vb, tmp_path):
+    """The shipped parameter scripts run the drop-in binaries with the
+    upstream flag set (values from the environment); --autotune=1 picks kernel
+    shapes on the first day and gives the untuned C to summation rounding."""
+    import os
+    run_dir = ROOT / "viss_optimize_ws_b200" / "run"
+    env = dict(os.environ, BTAG="1M", NSIDE="32", SEGS="4", SKY_DIR=str(tmp_path / "sky"), GPUS="0")
+    outs = {}
+    for tag, extra in (("plain", []), ("tuned", ["--autotune=1"])):
+        env["OUT_DIR"] = str(tmp_path / tag) + "/"
+        r = subprocess.run(["bash", str(run_dir / "main_recon_online_mirror_tile_vissfast.sh"), "--sky_gen=5", *extra],
+                           cwd=tmp_path, env=env, capture_output=True, text=True, timeout=600)
+        assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+        assert "exit code: 0" in r.stdout
+        assert ("Autotune:" in r.stdout) == bool(extra)
+        outs[tag] = np.fromfile(tmp_path / tag / "C1day1M.bin", dtype=np.float32)
+        assert outs[tag].size == 12 * 32 * 32
+    e = rel_err(outs["plain"], outs["tuned"])
+    assert e[0] < 2e-6 and e[1] < 2e-6, e
+    env["OUT_DIR"] = str(tmp_path / "root") + "/"
+    env["B_MODE"] = "bin"
+    r = subprocess.run(["bash", str(run_dir / "main_recon_online.sh"), "--sky_gen=5"], cwd=tmp_path,
+                       env=env, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    assert (tmp_path / "root" / "C1day1M.txt").exists() and (tmp_path / "root" / "Viss1day1M.txt").exists()

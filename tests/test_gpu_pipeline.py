@@ -139,3 +139,30 @@ def test_halfsym_violation_is_reported(gpu, vb):
         wp_, _ = p.ptr("w")
         rc = vb.lib().vb_validate_uvw_halfsym(ptr, vp_, wp_, n, p.nbl, C.byref(bad), None)
         assert rc == 6 and bad.value == 5
+
+
+def test_autotune_keeps_results_and_picks_a_valid_shape(gpu, vb):
+    """vb_pipeline_autotune times the kernel shapes on the pipeline's own
+    inputs, keeps the fastest, and the tuned run gives the untuned run's
+    results (to FP32 summation-order rounding; discrete W identical)."""
+    kw = dict(nside=32, orbit_model=vb.ORBIT_SYNTHETIC, nsat=8, tsteps=128, segs=4, lambda_m=30.0,
+              occ_R_m=6371e3, cull="tilecone", viss_tile_pix=1024, mirror=1, grid_res=257)
+    B = vb.synthetic_sky(32, seed=4)
+    with vb.Pipeline(vb.run_config(**kw)) as p:
+        p.set_sky(B)
+        p.make_baselines()
+        p.run()
+        C0, V0, W0 = p.get("C"), p.get("V_half"), p.get("W")
+        t = p.autotune(reps=1)
+        assert t["candidates"] >= 20
+        assert t["stage1_bpt"] in (1, 2, 4) and t["stage1_ctas_per_sm"] in (2, 3)
+        assert t["stage1_stage_pix"] in (256, 512, 1024) and t["stage2_ppt"] in (1, 2, 4)
+        assert 0 < t["stage1_ms"] <= t["stage1_default_ms"] and 0 < t["stage2_ms"] <= t["stage2_default_ms"]
+        r = p.run()
+        assert r["graph_kernels"] > 0 and r["error_flags"] == 0
+        C1, V1, W1 = p.get("C"), p.get("V_half"), p.get("W")
+        assert np.array_equal(W0, W1)
+        assert rel_err(V1, V0)[0] < 2e-6 and rel_err(C1, C0)[0] < 2e-6
+        # a second run of the tuned graph is bit-identical
+        p.run()
+        assert np.array_equal(p.get("C").view(np.uint32), C1.view(np.uint32))

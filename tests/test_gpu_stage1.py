@@ -210,6 +210,36 @@ def test_stage1_configs_and_determinism(case, vb):
         assert rel_err(Vc, Va)[0] < 2e-6
 
 
+@pytest.mark.parametrize("bpt,ctas,items", [(1, 3, 12), (2, 3, 48), (2, 2, 6), (4, 2, 24), (1, 2, 96)])
+@pytest.mark.parametrize("prec", ["fp32_fp64phase", "fp64"])
+def test_kernel_shapes_vs_fp64_oracle(case, vb, orc, bpt, ctas, items, prec):
+    """Every kernel shape the autotuner may pick (baselines per thread,
+    resident CTAs per SM, work granularity) gives the oracle's V, the same
+    term counters, and per-shape deterministic bits."""
+    c = case
+    sky, bl = structs(c)
+    pm = vb.PREC_FP64 if prec == "fp64" else vb.PREC_FP32_FP64PH
+    V, cnt = stage1(sky, bl, precision=pm, cull=vb.CULL_TILECONE, bpt=bpt, ctas_per_sm=ctas, items_per_cta=items)
+    V2, cnt2 = stage1(sky, bl, precision=pm, cull=vb.CULL_TILECONE, bpt=bpt, ctas_per_sm=ctas, items_per_cta=items)
+    assert np.array_equal(V.view(np.uint64), V2.view(np.uint64))
+    cls, _ = tile_classes(sky, bl, cull=vb.CULL_TILECONE)
+    Vo = orc.stage1(c["sky"], bl_dict(c), phase_corrected=1, tile_pix=256, tile_cls=cls, precision=1)
+    emax, erms = rel_err(V, Vo)
+    tol = TOL_FP64 if prec == "fp64" else TOL_MIXED
+    assert emax <= tol and erms <= tol, f"max {emax:.3e} rms {erms:.3e}"
+    # hidden and total terms are shape-independent; the visible / masked split
+    # is per warp (a warp takes the masked path when any of its baselines is mixed)
+    _, cnt0 = stage1(sky, bl, precision=pm, cull=vb.CULL_TILECONE)
+    assert cnt[2] == cnt0[2] and cnt[3] == cnt0[3] and cnt[0] + cnt[1] == cnt0[0] + cnt0[1]
+
+
+def test_kernel_shape_rejections(case, vb):
+    sky, bl = structs(case)
+    for kw in (dict(bpt=4, ctas_per_sm=3), dict(ctas_per_sm=5), dict(items_per_cta=-1), dict(bpt=3)):
+        o = vb.Stage1Opts(precision=vb.PREC_FP32_FP64PH, cull=vb.CULL_TILECONE, phase_corrected=1, blockage=1, **kw)
+        assert vb.lib().vb_stage1_workspace_bytes(C.byref(sky), C.byref(bl), C.byref(o)) == 0, kw
+
+
 def test_phase_correct_expand(case, vb, orc, ref):
     c = case
     nh = c["n_full"] // 2

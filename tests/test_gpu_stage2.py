@@ -160,10 +160,11 @@ def test_recon_vs_fp64_oracle(case, vb, orc, mirror, blockage, occ, prec):
 
 
 @pytest.mark.parametrize("ppt", [1, 2, 4])
-def test_recon_exact_block_culling_bit_identical(case, vb, ppt):
+def test_recon_exact_block_culling_matches_unculled(case, vb, ppt):
     """Exact pixel-block culling changes which groups take the per-pixel test,
-    never a result: C and W bit-identical to the unculled run at every block
-    size (256 * ppt pixels)."""
+    never which groups are included: W identical to the unculled run at every
+    block size (256 * ppt pixels); C equal up to the summation order (proven
+    visible groups are summed before the mixed ones)."""
     c = case
     proven = 0
     for pm in (vb.PREC_FP32_FP64PH, vb.PREC_FP32_DSPH, vb.PREC_FP64):
@@ -172,7 +173,9 @@ def test_recon_exact_block_culling_bit_identical(case, vb, ppt):
         C1, W1, _, k1 = stage2(c["sky"], c["bls"], c["dVh"], c["seg_t0"], c["seg_tlen"], precision=pm, cull=2,
                                lam=LAM, bl_max=BL_MAX, ppt=ppt)
         assert np.array_equal(W0, W1)
-        assert np.array_equal(C0.view(np.uint32), C1.view(np.uint32))
+        emax, erms = rel_err(C1, C0)
+        tol = 2e-7 if pm == vb.PREC_FP64 else 2e-6
+        assert emax <= tol and erms <= tol, (pm, emax, erms)
         assert int(k1[3]) == int(k0[3]) and int(k1[0] + k1[1] + k1[2]) == int(k1[3])
         proven += int(k1[0]) + int(k1[2]) - int(k0[2])
     if ppt == 1:

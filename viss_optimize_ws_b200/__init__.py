@@ -14,7 +14,7 @@ import ctypes as C
 import numpy as np
 
 from ._lib import (CULL_EXACT, CULL_NONE, CULL_TILECONE, ORBIT_REFERENCE, ORBIT_SYNTHETIC, PREC_FP32_DSPH,
-                   PREC_FP32_FP64PH, PREC_FP64, PREC_REF32, Baselines, DeviceBuffer, OrbitParams, Report,
+                   PREC_FP32_FP64PH, PREC_FP64, PREC_REF32, Baselines, DeviceBuffer, OrbitParams, Report, TuneReport,
                    RunConfig, SegParams, Sky, Stage1Opts, Stage2Opts, VbError, check, download, lib)
 
 __all__ = [
@@ -103,6 +103,13 @@ class Pipeline:
         r = Report()
         check(lib().vb_pipeline_run(self.h, C.byref(r)))
         return r.as_dict()
+
+    def autotune(self, reps: int = 2) -> dict:
+        """vb_pipeline_autotune: fastest kernel shapes for this workload, kept
+        in the pipeline's config."""
+        t = TuneReport()
+        check(lib().vb_pipeline_autotune(self.h, int(reps), C.byref(t)))
+        return t.as_dict()
 
     def run_host(self, B: np.ndarray, scale: bool = True, want_v: bool = False):
         B = np.ascontiguousarray(B, dtype=np.float32)

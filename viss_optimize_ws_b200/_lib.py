@@ -43,13 +43,14 @@ class Baselines(C.Structure):
 
 class Stage1Opts(C.Structure):
     _fields_ = [("precision", C.c_int), ("cull", C.c_int), ("phase_corrected", C.c_int), ("blockage", C.c_int),
-                ("bpt", C.c_int), ("stage_pix", C.c_int), ("chunk_pix", C.c_int), ("exact_tile_pix", C.c_int)]
+                ("bpt", C.c_int), ("stage_pix", C.c_int), ("chunk_pix", C.c_int), ("exact_tile_pix", C.c_int),
+                ("ctas_per_sm", C.c_int), ("items_per_cta", C.c_int)]
 
 
 class Stage2Opts(C.Structure):
     _fields_ = [("mirror", C.c_int), ("blockage", C.c_int), ("occ_mode", C.c_int), ("precision", C.c_int),
                 ("cull", C.c_int), ("grid_res", C.c_int), ("bl_max", C.c_float), ("lambda_", C.c_float),
-                ("ppt", C.c_int)]
+                ("ppt", C.c_int), ("items_per_cta", C.c_int)]
 
 
 class SegParams(C.Structure):
@@ -72,7 +73,9 @@ class RunConfig(C.Structure):
                 ("alt_min_km", C.c_double), ("alt_max_km", C.c_double), ("spread_km", C.c_double),
                 ("occ_R_m", C.c_double), ("bl_max_m", C.c_float), ("grid_res", C.c_int), ("seg_plan", C.c_int),
                 ("seg_min_half", C.c_int), ("seg_max_half", C.c_int), ("seg_seed", C.c_uint64),
-                ("stage2_cull", C.c_int), ("stage2_ppt", C.c_int), ("use_graph", C.c_int), ("device", C.c_int)]
+                ("stage2_cull", C.c_int), ("stage2_ppt", C.c_int), ("stage2_items_per_cta", C.c_int),
+                ("stage1_bpt", C.c_int), ("stage1_stage_pix", C.c_int), ("stage1_ctas_per_sm", C.c_int),
+                ("stage1_items_per_cta", C.c_int), ("use_graph", C.c_int), ("device", C.c_int)]
 
 
 class Report(C.Structure):
@@ -89,6 +92,22 @@ class Report(C.Structure):
         d["s1_counters"] = list(self.s1_counters)
         d["s2_counters"] = list(self.s2_counters)
         return d
+
+
+class TuneReport(C.Structure):
+    _fields_ = [("stage1_bpt", C.c_int), ("stage1_stage_pix", C.c_int), ("stage1_ctas_per_sm", C.c_int),
+                ("stage1_items_per_cta", C.c_int), ("stage2_ppt", C.c_int), ("stage2_items_per_cta", C.c_int),
+                ("stage1_ms", C.c_double), ("stage2_ms", C.c_double), ("stage1_default_ms", C.c_double),
+                ("stage2_default_ms", C.c_double), ("candidates", C.c_int)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+# ctypes mirror of each public struct, checked against vb_abi_sizeof
+ABI_STRUCTS = {"vb_sky": Sky, "vb_baselines": Baselines, "vb_stage1_opts": Stage1Opts, "vb_stage2_opts": Stage2Opts,
+               "vb_seg_params": SegParams, "vb_orbit_params": OrbitParams, "vb_run_config": RunConfig,
+               "vb_report": Report, "vb_tune_report": TuneReport}
 
 
 _SIGS = {
@@ -135,6 +154,8 @@ _SIGS = {
     "vb_pipeline_seg_plan": (C.c_int, [vp, vp, vp]),
     "vb_pipeline_seg_params": (C.c_int, [vp, vp]),
     "vb_pipeline_destroy": (C.c_int, [vp]),
+    "vb_pipeline_autotune": (C.c_int, [vp, C.c_int, C.POINTER(TuneReport)]),
+    "vb_abi_sizeof": (C.c_size_t, [C.c_char_p]),
     "vb_measure_peaks": (C.c_int, [C.POINTER(C.c_double)] * 4),
     "vb_flush_l2": (C.c_int, [vp, C.c_size_t, vp]),
     "vb_set_device": (C.c_int, [C.c_int]),

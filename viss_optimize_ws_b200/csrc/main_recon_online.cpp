@@ -187,6 +187,7 @@ int main(int argc, char** argv) {
   int use_graph = to_int(get_arg(argc, argv, "--graph", "1"), 1);
   std::string report_json = get_arg(argc, argv, "--report_json", "");
   int stage2_cull = to_int(get_arg(argc, argv, "--stage2_cull", "2"), 2);
+  int autotune = to_int(get_arg(argc, argv, "--autotune", "0"), 0);
 
   if (btag != "1M" && btag != "10M" && btag != "30M") return die("ERROR --btag");
   if (nside <= 0) nside = (btag == "1M") ? 512 : (btag == "10M" ? 4096 : 16384);
@@ -325,6 +326,22 @@ int main(int argc, char** argv) {
     int rc = vb_pipeline_make_baselines(p);
     if (rc == VB_ERR_HALFSYM) return die(std::string("ERROR: generated segment uvw does not satisfy half-sym: ") + vb_last_error());
     if (rc != VB_OK) return die(std::string("ERROR ") + vb_last_error());
+    if (autotune && di == 0) {
+      // kernel shapes for this workload, kept for the following days
+      vb_tune_report tr{};
+      if (vb_pipeline_autotune(p, 2, &tr) != VB_OK) return die(std::string("ERROR autotune: ") + vb_last_error());
+      cfg.stage1_bpt = tr.stage1_bpt;
+      cfg.stage1_stage_pix = tr.stage1_stage_pix;
+      cfg.stage1_ctas_per_sm = tr.stage1_ctas_per_sm;
+      cfg.stage1_items_per_cta = tr.stage1_items_per_cta;
+      cfg.stage2_ppt = tr.stage2_ppt;
+      cfg.stage2_items_per_cta = tr.stage2_items_per_cta;
+      std::cout << "Autotune: stage1 bpt=" << tr.stage1_bpt << " stage_pix=" << tr.stage1_stage_pix
+                << " ctas_per_sm=" << tr.stage1_ctas_per_sm << " items_per_cta=" << tr.stage1_items_per_cta << " "
+                << tr.stage1_ms << " ms (auto " << tr.stage1_default_ms << " ms); stage2 ppt=" << tr.stage2_ppt
+                << " items_per_cta=" << tr.stage2_items_per_cta << " " << tr.stage2_ms << " ms (auto "
+                << tr.stage2_default_ms << " ms); " << tr.candidates << " shapes timed\n";
+    }
     std::cout << "Init GPUs in " << t_init.toc_s() << " s\n";
     std::cout << "Orbit generator initialized on dev=0\n";
     std::cout << "Baseline broadcast: gen_dev=0 need_host_stage=0\n";

@@ -45,7 +45,7 @@ int geom_invnorm(const float* x, const float* y, const float* z, float* invn, in
 // ----- stage 1 ---------------------------------------------------------------
 struct Stage1Plan {
   int precision, cull, phase_corrected, blockage;
-  int bpt, stage_pix, chunk_pix, cull_tile;
+  int bpt, minb, stage_pix, chunk_pix, cull_tile;
   int64_t npix;
   int n_half, nbl;
   int nchunk, n_btile, n_items, grid;
@@ -81,8 +81,7 @@ struct Stage2Plan {
   int64_t npix;
   int block_pix;        // pixels per CTA
   int nblocks;          // pixel blocks
-  int gchunk;           // groups per item chunk
-  int max_gchunks;      // upper bound of group chunks
+  int nchunk_target;    // group chunks per pixel block (upper bound; sizes the partials)
   size_t cub_sort_bytes, cub_scan_bytes;
 };
 struct Stage2Pixels {       // pixel records already packed by the caller

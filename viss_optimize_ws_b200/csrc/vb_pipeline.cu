@@ -182,6 +182,36 @@ static void pipeline_free(vb_pipeline* p) {
   delete p;
 }
 
+// Frees one pipeline-owned device buffer.
+static void dfree(vb_pipeline* p, void* ptr) {
+  if (!ptr) return;
+  for (size_t i = 0; i < p->owned.size(); ++i)
+    if (p->owned[i] == ptr) {
+      cudaFree(ptr);
+      p->owned.erase(p->owned.begin() + (long)i);
+      return;
+    }
+}
+
+// Grows a pipeline-owned workspace to at least `need` bytes (contents lost).
+static int regrow(vb_pipeline* p, void** ws, size_t* cap, size_t need) {
+  if (*ws && *cap >= need) return VB_OK;
+  dfree(p, *ws);
+  *ws = nullptr;
+  *cap = 0;
+  VB_TRY(dalloc(p, reinterpret_cast<char**>(ws), need));
+  *cap = need;
+  return VB_OK;
+}
+
+static void drop_graph(vb_pipeline* p) {
+  if (p->gexec) cudaGraphExecDestroy(p->gexec);
+  if (p->graph) cudaGraphDestroy(p->graph);
+  p->gexec = nullptr;
+  p->graph = nullptr;
+  p->graph_kernels = 0;
+}
+
 static vb_sky sky_of(const vb_pipeline* p) {
   vb_sky k{};
   k.npix = p->npix;
@@ -250,6 +280,8 @@ static int uneven_total_steps(const vb_run_config& c, int nbl) {
   }
   return cur;
 }
+
+static int plan_stages(vb_pipeline* p);
 
 extern "C" int vb_pipeline_create(const vb_run_config* c, vb_pipeline** out) {
   if (!c || !out) return fail(VB_ERR_INVALID, "vb_pipeline_create: null argument");
@@ -351,36 +383,11 @@ extern "C" int vb_pipeline_create(const vb_run_config* c, vb_pipeline** out) {
     PTRY(dalloc(p, &p->cp2, p->n_full));
   }
 
-  // stage 1 plan + workspace
-  vb_sky sky = sky_of(p);
-  vb_baselines bl = bl_of(p);
-  vb_stage1_opts o1{};
-  o1.precision = c->precision;
-  o1.cull = c->cull;
-  o1.phase_corrected = 1;
-  o1.blockage = c->blockage;
-  PTRY(stage1_plan(&sky, &bl, &o1, &p->p1));
-  p->ws1_bytes = stage1_carve(p->p1, nullptr, 0, nullptr, true);
-  PTRY(dalloc(p, reinterpret_cast<char**>(&p->ws1), p->ws1_bytes));
-  stage1_carve(p->p1, p->ws1, p->ws1_bytes, &p->b1, true);
+  // stage plans + workspaces
+  PTRY(plan_stages(p));
   PTRY(dalloc(p, &p->Vd, (size_t)2 * p->n_half));
   PTRY(dalloc(p, &p->Vh, (size_t)2 * p->n_half));
   PTRY(dalloc(p, &p->Vf, (size_t)2 * p->n_full));
-
-  // stage 2 plan + workspace
-  vb_stage2_opts o2{};
-  o2.mirror = c->mirror;
-  o2.blockage = c->blockage;
-  o2.occ_mode = c->occ_mode;
-  o2.precision = c->precision;
-  o2.cull = c->stage2_cull;
-  o2.ppt = c->stage2_ppt;
-  o2.grid_res = c->grid_res;
-  o2.bl_max = c->bl_max_m;
-  o2.lambda = c->lambda_m;
-  PTRY(stage2_plan(p->n_half, p->nseg, p->npix, &o2, &p->p2));
-  p->ws2_bytes = stage2_workspace(p->p2, nullptr, 0, nullptr);
-  PTRY(dalloc(p, reinterpret_cast<char**>(&p->ws2), p->ws2_bytes));
   PTRY(dalloc(p, &p->C, p->npix));
   PTRY(dalloc(p, &p->W, p->npix));
   PTRY(dalloc(p, &p->segp, p->nseg));
@@ -456,6 +463,49 @@ static int enqueue_stages(vb_pipeline* p) {
   VB_TRY(stage2_run(&sky, &bl, p->Vh, p->nseg, p->d_t0, p->d_tlen, p->p2, p->ws2, p->ws2_bytes, p->C, p->W,
                     p->segp, p->counters + 4, p->wsum, p->s, &pre, p->ev[7], p->ev[8]));
   VB_CUDA(record_event(p->ev[2], p->s));
+  return VB_OK;
+}
+
+// Stage plans from the run config (kernel shapes included), workspaces grown
+// to fit them.  Any captured graph and the packed pixel records are rebuilt
+// by the next run.
+static int plan_stages(vb_pipeline* p) {
+  const vb_run_config* c = &p->cfg;
+  vb_sky sky = sky_of(p);
+  vb_baselines bl = bl_of(p);
+  vb_stage1_opts o1{};
+  o1.precision = c->precision;
+  o1.cull = c->cull;
+  o1.phase_corrected = 1;
+  o1.blockage = c->blockage;
+  o1.bpt = c->stage1_bpt;
+  o1.stage_pix = c->stage1_stage_pix;
+  o1.ctas_per_sm = c->stage1_ctas_per_sm;
+  o1.items_per_cta = c->stage1_items_per_cta;
+  Stage1Plan p1;
+  VB_TRY(stage1_plan(&sky, &bl, &o1, &p1));
+  vb_stage2_opts o2{};
+  o2.mirror = c->mirror;
+  o2.blockage = c->blockage;
+  o2.occ_mode = c->occ_mode;
+  o2.precision = c->precision;
+  o2.cull = c->stage2_cull;
+  o2.ppt = c->stage2_ppt;
+  o2.items_per_cta = c->stage2_items_per_cta;
+  o2.grid_res = c->grid_res;
+  o2.bl_max = c->bl_max_m;
+  o2.lambda = c->lambda_m;
+  Stage2Plan p2;
+  VB_TRY(stage2_plan(p->n_half, p->nseg, p->npix, &o2, &p2));
+  drop_graph(p);
+  if (p->s) VB_CUDA(cudaStreamSynchronize(p->s));
+  VB_TRY(regrow(p, &p->ws1, &p->ws1_bytes, stage1_carve(p1, nullptr, 0, nullptr, true)));
+  VB_TRY(regrow(p, &p->ws2, &p->ws2_bytes, stage2_workspace(p2, nullptr, 0, nullptr)));
+  p->p1 = p1;
+  p->p2 = p2;
+  stage1_carve(p->p1, p->ws1, p->ws1_bytes, &p->b1, true);
+  p->pixels_ready = false;
+  p->s2_cones_ready = false;
   return VB_OK;
 }
 
@@ -638,6 +688,108 @@ extern "C" int vb_pipeline_seg_params(vb_pipeline* p, vb_seg_params* out) {
   VB_CUDA(cudaStreamSynchronize(p->s));
   VB_CUDA(cudaMemcpy(out, p->segp, p->nseg * sizeof(vb_seg_params), cudaMemcpyDeviceToHost));
   return VB_OK;
+}
+
+// Both stages once, eagerly, on the current plans; kernel times of each stage.
+static int time_stages(vb_pipeline* p, int reps, double* k1, double* k2) {
+  VB_TRY(ensure_ready(p));
+  VB_TRY(enqueue_stages(p));   // warm-up (also builds the stage-2 block cones)
+  VB_CUDA(cudaStreamSynchronize(p->s));
+  p->s2_cones_ready = true;
+  double b1 = 1e300, b2 = 1e300;
+  for (int r = 0; r < reps; ++r) {
+    VB_TRY(enqueue_stages(p));
+    VB_CUDA(cudaStreamSynchronize(p->s));
+    float t1 = 0.f, t2 = 0.f;
+    VB_CUDA(cudaEventElapsedTime(&t1, p->ev[5], p->ev[6]));
+    VB_CUDA(cudaEventElapsedTime(&t2, p->ev[7], p->ev[8]));
+    b1 = std::min(b1, (double)t1);
+    b2 = std::min(b2, (double)t2);
+  }
+  *k1 = b1;
+  *k2 = b2;
+  return VB_OK;
+}
+
+extern "C" int vb_pipeline_autotune(vb_pipeline* p, int reps, vb_tune_report* out) {
+  if (!p) return fail(VB_ERR_INVALID, "vb_pipeline_autotune: null pipeline");
+  if (!p->sky_set) return fail(VB_ERR_INVALID, "vb_pipeline_autotune: sky not set");
+  VB_CUDA(cudaSetDevice(p->cfg.device));
+  if (reps <= 0) reps = 2;
+  vb_tune_report t{};
+  vb_run_config& c = p->cfg;
+  const vb_run_config start = c;
+  // the untuned (auto) shapes first
+  c.stage1_bpt = c.stage1_stage_pix = c.stage1_ctas_per_sm = c.stage1_items_per_cta = 0;
+  c.stage2_ppt = c.stage2_items_per_cta = 0;
+  int rc = plan_stages(p);
+  double k1 = 0, k2 = 0;
+  if (rc == VB_OK) rc = time_stages(p, reps, &k1, &k2);
+  if (rc != VB_OK) {
+    c = start;
+    plan_stages(p);
+    return rc;
+  }
+  t.stage1_default_ms = k1;
+  t.stage2_default_ms = k2;
+  double best1 = k1, best2 = k2;
+  int b_bpt = 0, b_stage = 0, b_ctas = 0, b_items1 = 0, b_ppt = 0, b_items2 = 0;
+  // stage 1: baselines per thread x staged pixels x resident CTAs x granularity
+  const int tile = (c.cull == VB_CULL_TILECONE) ? p->tile_pix : 1 << 30;
+  for (int bpt : {1, 2, 4})
+    for (int stage : {256, 512, 1024}) {
+      if (stage > tile) continue;
+      for (int ctas : {2, 3}) {
+        if (ctas == 3 && bpt > 2) continue;
+        for (int items : {12, 24, 48}) {
+          c.stage1_bpt = bpt; c.stage1_stage_pix = stage; c.stage1_ctas_per_sm = ctas; c.stage1_items_per_cta = items;
+          if (plan_stages(p) != VB_OK || time_stages(p, reps, &k1, &k2) != VB_OK) continue;
+          ++t.candidates;
+          if (k1 < best1) {
+            best1 = k1;
+            b_bpt = bpt; b_stage = stage; b_ctas = ctas; b_items1 = items;
+          }
+        }
+      }
+    }
+  c.stage1_bpt = b_bpt; c.stage1_stage_pix = b_stage; c.stage1_ctas_per_sm = b_ctas; c.stage1_items_per_cta = b_items1;
+  // stage 2: pixels per thread x granularity
+  for (int ppt : {1, 2, 4})
+    for (int items : {8, 16, 32, 64}) {
+      c.stage2_ppt = ppt; c.stage2_items_per_cta = items;
+      if (plan_stages(p) != VB_OK || time_stages(p, reps, &k1, &k2) != VB_OK) continue;
+      ++t.candidates;
+      if (k2 < best2) {
+        best2 = k2;
+        b_ppt = ppt; b_items2 = items;
+      }
+    }
+  c.stage2_ppt = b_ppt; c.stage2_items_per_cta = b_items2;
+  VB_TRY(plan_stages(p));
+  t.stage1_bpt = p->p1.bpt;
+  t.stage1_stage_pix = p->p1.stage_pix;
+  t.stage1_ctas_per_sm = p->p1.minb;
+  t.stage1_items_per_cta = b_items1;
+  t.stage2_ppt = p->p2.ppt;
+  t.stage2_items_per_cta = b_items2;
+  t.stage1_ms = best1;
+  t.stage2_ms = best2;
+  if (out) *out = t;
+  return VB_OK;
+}
+
+extern "C" size_t vb_abi_sizeof(const char* name) {
+  if (!name) return 0;
+  struct Entry { const char* n; size_t s; };
+  static const Entry table[] = {
+      {"vb_sky", sizeof(vb_sky)}, {"vb_baselines", sizeof(vb_baselines)},
+      {"vb_stage1_opts", sizeof(vb_stage1_opts)}, {"vb_stage2_opts", sizeof(vb_stage2_opts)},
+      {"vb_seg_params", sizeof(vb_seg_params)}, {"vb_orbit_params", sizeof(vb_orbit_params)},
+      {"vb_run_config", sizeof(vb_run_config)}, {"vb_report", sizeof(vb_report)},
+      {"vb_tune_report", sizeof(vb_tune_report)}};
+  for (const Entry& e : table)
+    if (std::strcmp(e.n, name) == 0) return e.s;
+  return 0;
 }
 
 extern "C" int vb_pipeline_destroy(vb_pipeline* p) {

@@ -181,8 +181,8 @@ __device__ constexpr float imag_sign() {
   return (MODE == VB_PREC_FP32_FP64PH || MODE == VB_PREC_FP32_DSPH) ? -1.0f : 1.0f;
 }
 
-template <int MODE, int BPT>
-__global__ void __launch_bounds__(S1_THREADS, 2) k_stage1(const S1Args a) {
+template <int MODE, int BPT, int MINB>
+__global__ void __launch_bounds__(S1_THREADS, MINB) k_stage1(const S1Args a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double2* s_lm = reinterpret_cast<double2*>(smem_raw);
   float4* s_nb = reinterpret_cast<float4*>(s_lm + a.stage_pix);
@@ -428,48 +428,30 @@ __global__ void k_phase_correct_expand(const double* __restrict__ Vr, const floa
 }
 
 // ---------------------------------------------------------------------------
-template <int MODE, int BPT>
-static int launch_mode(const S1Args& a, int grid, size_t smem, cudaStream_t s) {
-  auto kern = k_stage1<MODE, BPT>;
-  VB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  kern<<<grid, S1_THREADS, smem, s>>>(a);
-  VB_LAUNCH_CHECK();
-  return VB_OK;
+// Kernel variants: baselines per thread x the resident-CTA count the register
+// budget is built for (3 CTAs/SM = 80 registers, only with BPT <= 2).
+template <int MODE>
+static void* stage1_kernel(int bpt, int minb) {
+  if (bpt == 1) return minb == 3 ? (void*)k_stage1<MODE, 1, 3> : (void*)k_stage1<MODE, 1, 2>;
+  if (bpt == 2) return minb == 3 ? (void*)k_stage1<MODE, 2, 3> : (void*)k_stage1<MODE, 2, 2>;
+  return (void*)k_stage1<MODE, 4, 2>;
 }
 
-template <int MODE>
-static int launch_bpt(const S1Args& a, int bpt, int grid, size_t smem, cudaStream_t s) {
-  switch (bpt) {
-    case 1: return launch_mode<MODE, 1>(a, grid, smem, s);
-    case 2: return launch_mode<MODE, 2>(a, grid, smem, s);
-    case 4: return launch_mode<MODE, 4>(a, grid, smem, s);
-    default: return fail(VB_ERR_INVALID, "stage 1: bpt=%d (1, 2 or 4)", bpt);
+static void* stage1_kernel_of(int mode, int bpt, int minb) {
+  switch (mode) {
+    case VB_PREC_REF32: return stage1_kernel<VB_PREC_REF32>(bpt, minb);
+    case VB_PREC_FP64: return stage1_kernel<VB_PREC_FP64>(bpt, minb);
+    case VB_PREC_FP32_FP64PH: return stage1_kernel<VB_PREC_FP32_FP64PH>(bpt, minb);
+    default: return stage1_kernel<VB_PREC_FP32_DSPH>(bpt, minb);
   }
 }
 
-template <int MODE, int BPT>
-static int occupancy_of(size_t smem) {
+static int occupancy(int mode, int bpt, int minb, size_t smem) {
   int n = 0;
-  auto kern = k_stage1<MODE, BPT>;
+  const void* kern = stage1_kernel_of(mode, bpt, minb);
   if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 1;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, S1_THREADS, smem) != cudaSuccess) return 1;
   return n < 1 ? 1 : n;
-}
-
-static int occupancy(int mode, int bpt, size_t smem) {
-#define VB_OCC(M)                                          \
-  switch (bpt) {                                          \
-    case 1: return occupancy_of<M, 1>(smem);              \
-    case 2: return occupancy_of<M, 2>(smem);              \
-    default: return occupancy_of<M, 4>(smem);             \
-  }
-  switch (mode) {
-    case VB_PREC_REF32: VB_OCC(VB_PREC_REF32);
-    case VB_PREC_FP64: VB_OCC(VB_PREC_FP64);
-    case VB_PREC_FP32_FP64PH: VB_OCC(VB_PREC_FP32_FP64PH);
-    default: VB_OCC(VB_PREC_FP32_DSPH);
-  }
-#undef VB_OCC
 }
 
 static bool is_pow2(int x) { return x > 0 && (x & (x - 1)) == 0; }
@@ -489,6 +471,10 @@ int stage1_plan(const vb_sky* sky, const vb_baselines* bl, const vb_stage1_opts*
   q.blockage = o->blockage ? 1 : 0;
   q.bpt = o->bpt > 0 ? o->bpt : 2;
   if (q.bpt != 1 && q.bpt != 2 && q.bpt != 4) return fail(VB_ERR_INVALID, "stage 1: bpt=%d", q.bpt);
+  q.minb = o->ctas_per_sm > 0 ? o->ctas_per_sm : 2;
+  if (q.minb != 2 && !(q.minb == 3 && q.bpt <= 2))
+    return fail(VB_ERR_INVALID, "stage 1: ctas_per_sm=%d (2, or 3 with bpt <= 2)", o->ctas_per_sm);
+  if (o->items_per_cta < 0) return fail(VB_ERR_INVALID, "stage 1: items_per_cta=%d", o->items_per_cta);
   q.npix = sky->npix;
   q.n_half = bl->n_full / 2;
   q.nbl = bl->nbl;
@@ -516,10 +502,11 @@ int stage1_plan(const vb_sky* sky, const vb_baselines* bl, const vb_stage1_opts*
   const int per_tile = S1_THREADS * q.bpt;
   q.n_btile = (int)ceil_div(q.n_half, per_tile);
   size_t smem = (size_t)stage * 48;
-  int occ = occupancy(q.precision, q.bpt, smem);
+  int occ = occupancy(q.precision, q.bpt, q.minb, smem);
   int capacity = sm_count() * occ;
   q.grid = capacity;
-  int64_t target_items = (int64_t)capacity * 12;
+  // enough items per CTA that the dynamic queue's tail (one item) stays short
+  int64_t target_items = (int64_t)capacity * (o->items_per_cta > 0 ? o->items_per_cta : 24);
   int64_t nchunk = q.n_btile > 0 ? ceil_div(target_items, q.n_btile) : 1;
   int64_t max_chunks = ceil_div(q.npix, q.cull_tile);
   if (nchunk > max_chunks) nchunk = max_chunks;
@@ -585,13 +572,11 @@ int stage1_run(const vb_sky* sky, const vb_baselines* bl, const Stage1Plan& p, c
   a.queue = b.queue; a.partial = b.partial; a.counters = counters; a.err = b.err;
   VB_CUDA(cudaMemsetAsync(b.queue, 0, sizeof(int), s));
   size_t smem = (size_t)p.stage_pix * 48;
+  const void* kern = stage1_kernel_of(p.precision, p.bpt, p.minb);
+  VB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  void* args[] = {&a};
   if (kbeg) VB_CUDA(record_event(kbeg, s));
-  switch (p.precision) {
-    case VB_PREC_REF32: VB_TRY(launch_bpt<VB_PREC_REF32>(a, p.bpt, p.grid, smem, s)); break;
-    case VB_PREC_FP64: VB_TRY(launch_bpt<VB_PREC_FP64>(a, p.bpt, p.grid, smem, s)); break;
-    case VB_PREC_FP32_FP64PH: VB_TRY(launch_bpt<VB_PREC_FP32_FP64PH>(a, p.bpt, p.grid, smem, s)); break;
-    default: VB_TRY(launch_bpt<VB_PREC_FP32_DSPH>(a, p.bpt, p.grid, smem, s)); break;
-  }
+  VB_CUDA(cudaLaunchKernel(kern, dim3(p.grid), dim3(S1_THREADS), args, smem, s));
   if (kend) VB_CUDA(record_event(kend, s));
   int rg = (int)ceil_div(p.n_half, 256);
   if (rg > sm_count() * 16) rg = sm_count() * 16;

@@ -292,12 +292,20 @@ __global__ void k_group_records(const RecArgs r, int max_groups) {
 }
 
 // --- reconstruction ------------------------------------------------------------
+// Groups per work-queue chunk for ng groups split into at most nchunk_target
+// chunks (a multiple of the staging width): ceil(ng / result) <= nchunk_target.
+__host__ __device__ inline int group_chunk(int ng, int nchunk_target) {
+  int g = (ng + nchunk_target - 1) / nchunk_target;
+  g = (g + S2_STAGE - 1) / S2_STAGE * S2_STAGE;
+  return g < S2_STAGE ? S2_STAGE : g;
+}
+
 struct ReconArgs {
   const float4* f4;          // (l, m, n, B) per pixel
   const double2* lm;
   const float4* nb;          // (n as FP64 bits, B, nm1)
   int64_t npix;
-  int block_pix, nblocks, gchunk;
+  int block_pix, nblocks, nchunk_target;
   const int* ngroups;
   const GroupRec* rec;
   const GroupMeta* meta;
@@ -308,7 +316,7 @@ struct ReconArgs {
   int nbl, mirror, blockage, occ_mode, cull, finite_check;
   const ExactCone* cones;    // one per pixel block (cull == VB_CULL_EXACT)
   int* queue;
-  double* Cpart;             // [gchunk index][npix]
+  double* Cpart;             // [group chunk][npix]
   unsigned* Wpart;
   unsigned long long* counters;
   unsigned* err;
@@ -478,7 +486,8 @@ __global__ void __launch_bounds__(S2_THREADS, 2) k_recon_rec(const ReconArgs a) 
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
   const int ng = *a.ngroups;
-  const int nchunk = (ng + a.gchunk - 1) / a.gchunk;
+  const int gchunk = group_chunk(ng, a.nchunk_target);
+  const int nchunk = (ng + gchunk - 1) / gchunk;
   const int n_items = nchunk * a.nblocks;
   unsigned long long c_fast = 0, c_mask = 0, c_hid = 0, c_all = 0;
 
@@ -514,8 +523,8 @@ __global__ void __launch_bounds__(S2_THREADS, 2) k_recon_rec(const ReconArgs a) 
 #pragma unroll
     for (int q = 0; q < PPT; ++q) { totC[q] = 0.0; kc[q] = 0.f; totW[q] = 0u; }
 
-    const int g_begin = gc * a.gchunk;
-    const int g_end = min(ng, g_begin + a.gchunk);
+    const int g_begin = gc * gchunk;
+    const int g_end = min(ng, g_begin + gchunk);
     for (int gs = g_begin; gs < g_end; gs += S2_STAGE) {
       const int nst = min(S2_STAGE, g_end - gs);
       __syncthreads();   // previous stage's lists fully read; s_cone visible
@@ -649,7 +658,8 @@ __global__ void __launch_bounds__(S2_THREADS) k_recon_members(const ReconArgs a)
   __shared__ int s_item;
   constexpr bool kDouble = (MODE == VB_PREC_FP64);
   const int ng = *a.ngroups;
-  const int nchunk = (ng + a.gchunk - 1) / a.gchunk;
+  const int gchunk = group_chunk(ng, a.nchunk_target);
+  const int nchunk = (ng + gchunk - 1) / gchunk;
   const int n_items = nchunk * a.nblocks;
   unsigned long long c_all = 0;
   for (;;) {
@@ -675,8 +685,8 @@ __global__ void __launch_bounds__(S2_THREADS) k_recon_members(const ReconArgs a)
     const int npx_blk = (int)min((int64_t)a.block_pix, a.npix - (int64_t)blk * a.block_pix);
     double totC = 0.0;
     unsigned totW = 0;
-    const int g_begin = gc * a.gchunk;
-    const int g_end = min(ng, g_begin + a.gchunk);
+    const int g_begin = gc * gchunk;
+    const int g_end = min(ng, g_begin + gchunk);
     for (int gs = g_begin; gs < g_end; gs += S2_STAGE) {
       const int nst = min(S2_STAGE, g_end - gs);
       __syncthreads();
@@ -744,9 +754,10 @@ __global__ void __launch_bounds__(S2_THREADS) k_recon_members(const ReconArgs a)
 }
 
 __global__ void k_finalize(const double* __restrict__ Cpart, const unsigned* __restrict__ Wpart,
-                           const int* __restrict__ ngroups, int gchunk, int64_t npix, int blockage,
+                           const int* __restrict__ ngroups, int nchunk_target, int64_t npix, int blockage,
                            float* __restrict__ C, uint32_t* __restrict__ W, double* __restrict__ wsum_out) {
   const int ng = *ngroups;
+  const int gchunk = group_chunk(ng, nchunk_target);
   const int nchunk = (ng + gchunk - 1) / gchunk;
   if (blockIdx.x == 0 && threadIdx.x == 0 && wsum_out) *wsum_out = (double)ng;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
@@ -794,16 +805,18 @@ int stage2_plan(int n_half_total, int nseg, int64_t npix, const vb_stage2_opts* 
   q.npix = npix;
   q.block_pix = S2_THREADS * q.ppt;
   q.nblocks = (int)ceil_div(npix, q.block_pix);
+  if (o->items_per_cta < 0) return fail(VB_ERR_INVALID, "stage 2: items_per_cta=%d", o->items_per_cta);
   const int capacity = sm_count() * 2;
-  const int64_t want_items = (int64_t)capacity * 8;
+  // enough items per CTA that the dynamic queue's tail (one item) stays short
+  const int64_t want_items = (int64_t)capacity * (o->items_per_cta > 0 ? o->items_per_cta : 24);
   int64_t nchunks = ceil_div(want_items, q.nblocks);
   if (nchunks < 1) nchunks = 1;
-  int64_t gchunk = ceil_div(q.n_keyed_total > 0 ? q.n_keyed_total : 1, nchunks);
-  gchunk = ceil_div(gchunk, S2_STAGE) * S2_STAGE;
-  if (gchunk < S2_STAGE) gchunk = S2_STAGE;
-  q.gchunk = (int)gchunk;
-  q.max_gchunks = (int)ceil_div(q.n_keyed_total > 0 ? q.n_keyed_total : 1, gchunk);
-  if ((int64_t)q.nblocks * q.max_gchunks > INT32_MAX) return fail(VB_ERR_UNSUPPORTED, "stage 2: too many work items");
+  // the group count is known on the device only: the kernels split it into at
+  // most nchunk_target chunks (group_chunk), which sizes the partial buffers
+  const int64_t max_useful = ceil_div(q.n_keyed_total > 0 ? q.n_keyed_total : 1, S2_STAGE);
+  if (nchunks > max_useful) nchunks = max_useful;
+  q.nchunk_target = (int)nchunks;
+  if ((int64_t)q.nblocks * q.nchunk_target > INT32_MAX) return fail(VB_ERR_UNSUPPORTED, "stage 2: too many work items");
   // CUB temporary storage for the largest batch
   size_t sort_bytes = 0, scan_bytes = 0;
   int n = q.n_keyed_total > 0 ? q.n_keyed_total : 1;
@@ -856,8 +869,8 @@ static size_t carve2(const Stage2Plan& p, void* ws, size_t cap, S2Slices* s) {
   x.wsum = c.take<double>(2);
   x.rec = c.take<GroupRec>(n);
   x.meta = c.take<GroupMeta>(n);
-  x.Cpart = c.take<double>((size_t)p.max_gchunks * (size_t)p.npix);
-  x.Wpart = c.take<unsigned>((size_t)p.max_gchunks * (size_t)p.npix);
+  x.Cpart = c.take<double>((size_t)p.nchunk_target * (size_t)p.npix);
+  x.Wpart = c.take<unsigned>((size_t)p.nchunk_target * (size_t)p.npix);
   x.cones = c.take<ExactCone>(p.nblocks);
   x.lm = c.take<double2>(p.npix);
   x.nb = c.take<float4>(p.npix);
@@ -979,7 +992,7 @@ int stage2_run(const vb_sky* sky, const vb_baselines* bl, const float* V_half, i
   if (n > 0) {
     ReconArgs ra{};
     ra.f4 = pf4; ra.lm = plm; ra.nb = pnb; ra.npix = p.npix;
-    ra.block_pix = p.block_pix; ra.nblocks = p.nblocks; ra.gchunk = p.gchunk;
+    ra.block_pix = p.block_pix; ra.nblocks = p.nblocks; ra.nchunk_target = p.nchunk_target;
     ra.ngroups = x.ngroups; ra.rec = x.rec; ra.meta = x.meta; ra.svals = sv; ra.V = Vk;
     ra.x1 = bl->x1; ra.y1 = bl->y1; ra.z1 = bl->z1; ra.in1 = bl->invn1;
     ra.x2 = bl->x2; ra.y2 = bl->y2; ra.z2 = bl->z2; ra.in2 = bl->invn2;
@@ -1005,7 +1018,7 @@ int stage2_run(const vb_sky* sky, const vb_baselines* bl, const float* V_half, i
   // 9. finalize: sum the group-chunk partials, normalise
   int gf = (int)ceil_div(p.npix, 256);
   if (gf > sm_count() * 16) gf = sm_count() * 16;
-  k_finalize<<<gf, 256, 0, st>>>(x.Cpart, x.Wpart, x.ngroups, p.gchunk, p.npix, p.blockage, C, W, x.wsum);
+  k_finalize<<<gf, 256, 0, st>>>(x.Cpart, x.Wpart, x.ngroups, p.nchunk_target, p.npix, p.blockage, C, W, x.wsum);
   VB_LAUNCH_CHECK();
   if (seg_params_out)
     VB_CUDA(cudaMemcpyAsync(seg_params_out, x.sp, nseg * sizeof(vb_seg_params), cudaMemcpyDeviceToDevice, st));
