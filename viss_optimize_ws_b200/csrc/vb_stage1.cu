@@ -19,8 +19,8 @@
 //   REF32  : FP32 phase (upstream arithmetic), FP32 sincos, FP32 stage sums.
 //   FP64   : FP64 phase, FP64 sincos, FP64 sums (the plain FP64 direct sum).
 //   F32X   : phase formed in FP64 with a magic-constant range reduction: the
-//            turn fraction lands in the low word of the double; its top 23
-//            bits become an exact FP32 angle in [0, 2pi); FP32 sincos; FP32
+//            turn fraction lands in the low 23 bits of the double and becomes
+//            an exact FP32 angle in [0, 2pi); FP32 sincos; FP32
 //            sums per staged tile (<= 1024 terms), FP64 across tiles.
 //   DS     : each product split exactly (p = fl(a b), e = fma(a, b, -p)),
 //            fractions p - rint(p) exact in FP32; FP32 sincos; Kahan sums
@@ -38,15 +38,15 @@ namespace vb {
 constexpr int S1_THREADS = 256;
 constexpr int kClsHid = 0, kClsVis = 1, kClsMix = 2;
 
-// F32X phase reduction: magic = 1.5 * 2^23 keeps every partial sum of the FMA
-// chain in [2^23, 2^24) while 4*max|uvw| < 2^22; the double's ulp is then
-// 2^-29 turns and bits [6, 29) of the low word are the top 23 fraction bits.
-constexpr double kMagic = 12582912.0;              // 1.5 * 2^23
-constexpr double kHalfLsb = 5.9604644775390625e-8; // 2^-24 turns: rounds the truncation
-constexpr int kFracShift = 6;
+// F32X phase reduction: magic = 1.5 * 2^29 keeps every partial sum of the FMA
+// chain in [2^29, 2^30) (|u| + |v| + |w| < 2^28); the double's ulp is then
+// 2^-23 turns, so each FMA rounds to nearest on the 2^-23-turn grid the FP32
+// angle is built on, and the low 23 bits of the double are the turn fraction:
+// one LOP3 turns them into the exact float 2^23 + k.
+constexpr double kMagic = 805306368.0;              // 1.5 * 2^29
 constexpr float kTwoPiF = 6.28318530717958647692f;
 constexpr float kAngScale = 6.28318530717958647692f * 1.1920928955078125e-7f;  // fl(2pi) * 2^-23
-constexpr double kMaxUvwF32X = 1048576.0;          // 2^20
+constexpr double kMaxUvwF32X = 67108864.0;         // 2^26: 3 * 2^26 < 2^28
 
 struct S1Args {
   const double2* __restrict__ lm;
@@ -110,7 +110,7 @@ __device__ __forceinline__ void load_baseline(const S1Args& a, int ih, bool raw,
   float uu = b.active ? a.u[i] : 0.f, vv = b.active ? a.v[i] : 0.f, ww = b.active ? a.w[i] : 0.f;
   b.uf = uu; b.vf = vv; b.wf = ww;
   b.U = uu; b.V = vv; b.W = ww;
-  b.C = kMagic + kHalfLsb - (raw ? (double)ww : 0.0);
+  b.C = kMagic - (raw ? (double)ww : 0.0);
   b.fw = raw ? -__fsub_rn(ww, rint_magic(ww)) : 0.0f;
   const float kk = -2.0f * 3.14159265358979323846f;
   b.ku = kk * uu; b.kv = kk * vv; b.kw = kk * ww;
@@ -145,8 +145,8 @@ __device__ __forceinline__ void phase_sincos(const Baseline& b, const double2 lm
   if constexpr (MODE == VB_PREC_FP32_FP64PH) {
     double t = fma(b.U, lm.x, fma(b.V, lm.y, fma(b.W, nd, b.C)));
     unsigned lo = (unsigned)__double2loint(t);
-    if constexpr (PAR) lo ^= 1u << (kFracShift + 22);   // + 1/2 turn (top fraction bit)
-    unsigned kb = ((lo >> kFracShift) & 0x7FFFFFu) | 0x4B000000u;
+    if constexpr (PAR) lo ^= 1u << 22;   // + 1/2 turn (top fraction bit)
+    unsigned kb = (lo & 0x7FFFFFu) | 0x4B000000u;
     float ang = __fmaf_rn(__uint_as_float(kb), kAngScale, -kTwoPiF);
     __sincosf(ang, &s, &c);
   } else if constexpr (MODE == VB_PREC_FP32_DSPH) {

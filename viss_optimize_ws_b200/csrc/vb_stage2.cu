@@ -29,9 +29,7 @@ namespace vb {
 
 constexpr int S2_THREADS = 256;
 constexpr int S2_STAGE = S2_THREADS;     // group records staged per step (one per thread)
-constexpr double kMagic2 = 12582912.0;   // 1.5 * 2^23, see stage 1
-constexpr double kHalfLsb2 = 5.9604644775390625e-8;
-constexpr int kFracShift2 = 6;
+constexpr double kMagic2 = 805306368.0;  // 1.5 * 2^29: 2^-23-turn ulp, see stage 1
 constexpr float kTwoPiF2 = 6.28318530717958647692f;
 constexpr float kAngScale2 = 6.28318530717958647692f * 1.1920928955078125e-7f;
 
@@ -261,7 +259,8 @@ __global__ void k_group_records(const RecArgs r, int max_groups) {
     o.clo = (float)(o.c - (double)o.chi);
     o.fa = q.fa;
     o.fb = q.fb;
-    if (fabs(o.a) + fabs(o.b) + fabs(o.c) >= 4194304.0) atomicOr(r.err, ERR_BAD_INDEX);
+    // the F32X phase needs |a l + b m + c n| < 2^28 turns (kMagic2)
+    if (fabs(o.a) + fabs(o.b) + fabs(o.c) >= 268435456.0) atomicOr(r.err, ERR_BAD_INDEX);
     o.vx = o.vy = 0.f;
     o.cp1 = o.cp2 = r.cosphi;
     o.p1 = o.p2 = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -326,9 +325,9 @@ template <int MODE>
 __device__ __forceinline__ void recon_phase(const GroupRec& g, double ld, double md, double nd, float lf, float mf,
                                             float nf, float& s, float& c, double& sd, double& cd) {
   if constexpr (MODE == VB_PREC_FP32_FP64PH) {
-    double t = fma(g.a, ld, fma(g.b, md, fma(g.c, nd, kMagic2 + kHalfLsb2)));
+    double t = fma(g.a, ld, fma(g.b, md, fma(g.c, nd, kMagic2)));
     unsigned lo = (unsigned)__double2loint(t);
-    unsigned kb = ((lo >> kFracShift2) & 0x7FFFFFu) | 0x4B000000u;
+    unsigned kb = (lo & 0x7FFFFFu) | 0x4B000000u;
     float ang = __fmaf_rn(__uint_as_float(kb), kAngScale2, -kTwoPiF2);
     __sincosf(ang, &s, &c);
   } else if constexpr (MODE == VB_PREC_FP32_DSPH) {
@@ -418,10 +417,10 @@ struct RecPix {
 template <int MODE, int PAR, class Acc>
 __device__ __forceinline__ void rec_term(const TermRec<MODE>& r, const RecPix& p, Acc& acc) {
   if constexpr (MODE == VB_PREC_FP32_FP64PH) {
-    constexpr double K = kMagic2 + kHalfLsb2 + (PAR ? 0.5 : 0.0);
+    constexpr double K = kMagic2 + (PAR ? 0.5 : 0.0);
     const double t = fma(r.a, p.ld, fma(r.b, p.md, fma(r.c, p.nd, K)));
     const unsigned lo = (unsigned)__double2loint(t);
-    const unsigned kb = ((lo >> kFracShift2) & 0x7FFFFFu) | 0x4B000000u;
+    const unsigned kb = (lo & 0x7FFFFFu) | 0x4B000000u;
     const float ang = __fmaf_rn(__uint_as_float(kb), kAngScale2, -kTwoPiF2);
     float s, c;
     __sincosf(ang, &s, &c);
