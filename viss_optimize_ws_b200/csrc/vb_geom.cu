@@ -200,10 +200,12 @@ k_exact_cone_meta(int tile_pix, const float* __restrict__ l, const float* __rest
       __syncthreads();
     }
     if (t == 0) {
-      double alpha = acos(fmax(-1.0, fmin(1.0, rx[0]))) + 1e-9;
+      const double alpha = acos(fmax(-1.0, fmin(1.0, rx[0]))) + 1e-9;
       ExactCone e;
       e.cx = ccx; e.cy = ccy; e.cz = ccz;
-      e.alpha = alpha;
+      e.cos_a = cos(alpha);
+      e.sin_a = sin(alpha);
+      e.pad = 0.0;
       out[tile] = e;
     }
     __syncthreads();

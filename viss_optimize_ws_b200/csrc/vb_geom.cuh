@@ -74,9 +74,12 @@ __device__ __forceinline__ int exact_class(const ExactCone& c, float x, float y,
   double rn = sqrt(rx * rx + ry * ry + rz * rz);
   double cd = (c.cx * rx + c.cy * ry + c.cz * rz) / rn;
   cd = fmin(1.0, fmax(-1.0, cd));
-  double d = acos(cd);
-  double lo = (d + c.alpha >= 3.141592653589793) ? -1.0 : cos(d + c.alpha);
-  double hi = (d <= c.alpha) ? 1.0 : cos(d - c.alpha);
+  // d = angle(axis, endpoint), a = half-angle: the cone's dots with the
+  // endpoint span [cos(d + a), cos(d - a)], clamped at d + a >= pi and d <= a;
+  // cos(d -/+ a) = cos d cos a +/- sin d sin a with sin d = sqrt(1 - cos^2 d)
+  const double sd = sqrt(fmax(0.0, 1.0 - cd * cd));
+  double lo = (cd <= -c.cos_a) ? -1.0 : cd * c.cos_a - sd * c.sin_a;
+  double hi = (cd >= c.cos_a) ? 1.0 : cd * c.cos_a + sd * c.sin_a;
   // scale by the endpoint norm (|r invn| = 1 +- 3e-7) conservatively
   const double margin = 1e-5;
   if (lo * rn - margin >= (double)cosphi && lo - margin >= (double)cosphi) return 1;

@@ -9,8 +9,8 @@ namespace vb {
 
 // Conservative pixel-tile cone (FP64): unit centre and the largest angle
 // between the centre and any pixel of the tile.
-struct ExactCone {
-  double cx, cy, cz, alpha;
+struct ExactCone {          // unit axis and cos / sin of the half-angle
+  double cx, cy, cz, cos_a, sin_a, pad;
 };
 
 // One satellite of the synthetic formation (circular orbit).

@@ -79,27 +79,44 @@ __device__ __forceinline__ float rint_magic(float x) {
   return __fsub_rn(__fadd_rn(x, 12582912.0f), 12582912.0f);
 }
 
+// VB_CULL_EXACT class of one baseline for one tile.  Kept out of line: the
+// FP64 cone test runs once per (baseline, tile), and inlining it into the
+// persistent kernel costs the pixel loop registers in every cull mode.
+__device__ __noinline__ int exact_tile_class(const ExactCone* cone, float x1, float y1, float z1, float i1, float c1,
+                                             float x2, float y2, float z2, float i2, float c2) {
+  const ExactCone c = *cone;
+  const int e1 = exact_class(c, x1, y1, z1, i1, c1);
+  const int e2 = exact_class(c, x2, y2, z2, i2, c2);
+  return (e1 < 0 || e2 < 0) ? kClsHid : ((e1 > 0 && e2 > 0) ? kClsVis : kClsMix);
+}
+
 // Tile class of one baseline for one cull tile (0 hidden, 1 visible, 2 mixed).
 // Upstream decision: ..._vissfast.cuh:519-531 (tile cone), per-pixel mask
-// everywhere for the plain kernel (viss_recon_kernel.cuh:270-274).
+// everywhere for the plain kernel (viss_recon_kernel.cuh:270-274).  The cull
+// mode is a template argument so that each mode's kernel carries only its own
+// test.
+template <int CULL>
 __device__ __forceinline__ int tile_class(const S1Args& a, const Baseline& b, int tile_id) {
   if (!b.active) return kClsHid;
   if (!a.blockage) return kClsVis;
-  if (a.cull == VB_CULL_TILECONE) {
+  if constexpr (CULL == VB_CULL_TILECONE) {
     const float cx = a.tcx[tile_id], cy = a.tcy[tile_id], cz = a.tcz[tile_id];
     const float cA = a.tcosA[tile_id], sA = a.tsinA[tile_id];
     bool vis1, hid1, vis2, hid2;
     cone_classify(cone_dot(b.ux1, b.uy1, b.uz1, cx, cy, cz), cA, sA, b.c1, vis1, hid1);
     cone_classify(cone_dot(b.ux2, b.uy2, b.uz2, cx, cy, cz), cA, sA, b.c2, vis2, hid2);
     return (hid1 || hid2) ? kClsHid : ((vis1 && vis2) ? kClsVis : kClsMix);
+  } else if constexpr (CULL == VB_CULL_EXACT) {
+    return exact_tile_class(a.cones + tile_id, b.x1, b.y1, b.z1, b.i1, b.c1, b.x2, b.y2, b.z2, b.i2, b.c2);
+  } else {
+    return kClsMix;
   }
-  if (a.cull == VB_CULL_EXACT) {
-    const ExactCone c = a.cones[tile_id];
-    int e1 = exact_class(c, b.x1, b.y1, b.z1, b.i1, b.c1);
-    int e2 = exact_class(c, b.x2, b.y2, b.z2, b.i2, b.c2);
-    return (e1 < 0 || e2 < 0) ? kClsHid : ((e1 > 0 && e2 > 0) ? kClsVis : kClsMix);
-  }
-  return kClsMix;
+}
+
+__device__ __forceinline__ int tile_class_rt(const S1Args& a, const Baseline& b, int tile_id) {
+  if (a.cull == VB_CULL_TILECONE) return tile_class<VB_CULL_TILECONE>(a, b, tile_id);
+  if (a.cull == VB_CULL_EXACT) return tile_class<VB_CULL_EXACT>(a, b, tile_id);
+  return tile_class<VB_CULL_NONE>(a, b, tile_id);
 }
 
 // Loads half-baseline ih into registers (upstream: viss_recon_kernel.cuh:231-240,
@@ -181,8 +198,11 @@ __device__ constexpr float imag_sign() {
   return (MODE == VB_PREC_FP32_FP64PH || MODE == VB_PREC_FP32_DSPH) ? -1.0f : 1.0f;
 }
 
-template <int MODE, int BPT, int MINB>
-__global__ void __launch_bounds__(S1_THREADS, MINB) k_stage1(const S1Args a) {
+// Register budget per thread: 80 for 3 resident CTAs of 256 threads; 120 for
+// 2 (measured: 120 beats the full 128 the 2-CTA budget allows by ~2 % on the
+// nside-256 workload, 112 and below lose more to the extra scheduling limits).
+template <int MODE, int BPT, int MINB, int CULL>
+__global__ void __maxnreg__(MINB == 3 ? 80 : 120) k_stage1(const S1Args a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double2* s_lm = reinterpret_cast<double2*>(smem_raw);
   float4* s_nb = reinterpret_cast<float4*>(s_lm + a.stage_pix);
@@ -244,7 +264,7 @@ __global__ void __launch_bounds__(S1_THREADS, MINB) k_stage1(const S1Args a) {
 #pragma unroll
       for (int k = 0; k < BPT; ++k) {
         Baseline& b = bl[k];
-        const int cls = tile_class(a, b, tile_id);
+        const int cls = tile_class<CULL>(a, b, tile_id);
         b.cls = cls;
         any_live |= (cls != kClsHid);
         any_mix |= (cls == kClsMix);
@@ -428,27 +448,35 @@ __global__ void k_phase_correct_expand(const double* __restrict__ Vr, const floa
 }
 
 // ---------------------------------------------------------------------------
-// Kernel variants: baselines per thread x the resident-CTA count the register
-// budget is built for (3 CTAs/SM = 80 registers, only with BPT <= 2).
-template <int MODE>
+// Kernel variants: precision x cull mode x baselines per thread x the
+// resident-CTA count the register budget is built for (3 CTAs/SM = 80
+// registers, only with BPT <= 2).
+template <int MODE, int CULL>
 static void* stage1_kernel(int bpt, int minb) {
-  if (bpt == 1) return minb == 3 ? (void*)k_stage1<MODE, 1, 3> : (void*)k_stage1<MODE, 1, 2>;
-  if (bpt == 2) return minb == 3 ? (void*)k_stage1<MODE, 2, 3> : (void*)k_stage1<MODE, 2, 2>;
-  return (void*)k_stage1<MODE, 4, 2>;
+  if (bpt == 1) return minb == 3 ? (void*)k_stage1<MODE, 1, 3, CULL> : (void*)k_stage1<MODE, 1, 2, CULL>;
+  if (bpt == 2) return minb == 3 ? (void*)k_stage1<MODE, 2, 3, CULL> : (void*)k_stage1<MODE, 2, 2, CULL>;
+  return (void*)k_stage1<MODE, 4, 2, CULL>;
 }
 
-static void* stage1_kernel_of(int mode, int bpt, int minb) {
+template <int MODE>
+static void* stage1_kernel_cull(int bpt, int minb, int cull) {
+  if (cull == VB_CULL_TILECONE) return stage1_kernel<MODE, VB_CULL_TILECONE>(bpt, minb);
+  if (cull == VB_CULL_EXACT) return stage1_kernel<MODE, VB_CULL_EXACT>(bpt, minb);
+  return stage1_kernel<MODE, VB_CULL_NONE>(bpt, minb);
+}
+
+static void* stage1_kernel_of(int mode, int bpt, int minb, int cull) {
   switch (mode) {
-    case VB_PREC_REF32: return stage1_kernel<VB_PREC_REF32>(bpt, minb);
-    case VB_PREC_FP64: return stage1_kernel<VB_PREC_FP64>(bpt, minb);
-    case VB_PREC_FP32_FP64PH: return stage1_kernel<VB_PREC_FP32_FP64PH>(bpt, minb);
-    default: return stage1_kernel<VB_PREC_FP32_DSPH>(bpt, minb);
+    case VB_PREC_REF32: return stage1_kernel_cull<VB_PREC_REF32>(bpt, minb, cull);
+    case VB_PREC_FP64: return stage1_kernel_cull<VB_PREC_FP64>(bpt, minb, cull);
+    case VB_PREC_FP32_FP64PH: return stage1_kernel_cull<VB_PREC_FP32_FP64PH>(bpt, minb, cull);
+    default: return stage1_kernel_cull<VB_PREC_FP32_DSPH>(bpt, minb, cull);
   }
 }
 
-static int occupancy(int mode, int bpt, int minb, size_t smem) {
+static int occupancy(int mode, int bpt, int minb, int cull, size_t smem) {
   int n = 0;
-  const void* kern = stage1_kernel_of(mode, bpt, minb);
+  const void* kern = stage1_kernel_of(mode, bpt, minb, cull);
   if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 1;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, S1_THREADS, smem) != cudaSuccess) return 1;
   return n < 1 ? 1 : n;
@@ -502,7 +530,7 @@ int stage1_plan(const vb_sky* sky, const vb_baselines* bl, const vb_stage1_opts*
   const int per_tile = S1_THREADS * q.bpt;
   q.n_btile = (int)ceil_div(q.n_half, per_tile);
   size_t smem = (size_t)stage * 48;
-  int occ = occupancy(q.precision, q.bpt, q.minb, smem);
+  int occ = occupancy(q.precision, q.bpt, q.minb, q.cull, smem);
   int capacity = sm_count() * occ;
   q.grid = capacity;
   // enough items per CTA that the dynamic queue's tail (one item) stays short
@@ -572,7 +600,7 @@ int stage1_run(const vb_sky* sky, const vb_baselines* bl, const Stage1Plan& p, c
   a.queue = b.queue; a.partial = b.partial; a.counters = counters; a.err = b.err;
   VB_CUDA(cudaMemsetAsync(b.queue, 0, sizeof(int), s));
   size_t smem = (size_t)p.stage_pix * 48;
-  const void* kern = stage1_kernel_of(p.precision, p.bpt, p.minb);
+  const void* kern = stage1_kernel_of(p.precision, p.bpt, p.minb, p.cull);
   VB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   void* args[] = {&a};
   if (kbeg) VB_CUDA(record_event(kbeg, s));
@@ -644,7 +672,7 @@ __global__ void k_tile_classes(const S1Args a, int ntile, uint8_t* __restrict__ 
     const int t = (int)(q - (int64_t)ih * ntile);
     Baseline b;
     load_baseline(a, ih, raw, b);
-    cls[q] = (uint8_t)tile_class(a, b, t);
+    cls[q] = (uint8_t)tile_class_rt(a, b, t);
   }
 }
 }  // namespace vb

@@ -462,6 +462,16 @@ __device__ __forceinline__ void rec_term(const TermRec<MODE>& r, const RecPix& p
   }
 }
 
+// Exact-cone class of a representative against a pixel block (0 hidden,
+// 1 visible, 2 mixed).  Out of line: it runs once per (group, block) and would
+// otherwise take registers from the term loop.
+__device__ __noinline__ int exact_group_class(const ExactCone* cone, float4 p1, float cp1, float4 p2, float cp2) {
+  const ExactCone c = *cone;
+  const int e1 = exact_class(c, p1.x, p1.y, p1.z, p1.w, cp1);
+  const int e2 = exact_class(c, p2.x, p2.y, p2.z, p2.w, cp2);
+  return (e1 < 0 || e2 < 0) ? 0 : ((e1 > 0 && e2 > 0) ? 1 : 2);
+}
+
 // occ_mode 2 (representative) and blockage=0 (group averages) paths.
 //
 // Work item = (pixel block of PPT * 256 pixels, chunk of groups).  Each thread
@@ -535,9 +545,7 @@ __global__ void __launch_bounds__(S2_THREADS, 2) k_recon_rec(const ReconArgs a) 
         if (r.flags & 3) cls = 0;              // key 0, or non-finite V: neither summed nor counted
         else if (!a.blockage) cls = 1;
         else if (a.cull == VB_CULL_EXACT) {
-          const int e1 = exact_class(s_cone, r.p1.x, r.p1.y, r.p1.z, r.p1.w, r.cp1);
-          const int e2 = exact_class(s_cone, r.p2.x, r.p2.y, r.p2.z, r.p2.w, r.cp2);
-          cls = (e1 < 0 || e2 < 0) ? 0 : ((e1 > 0 && e2 > 0) ? 1 : 2);
+          cls = exact_group_class(&s_cone, r.p1, r.cp1, r.p2, r.cp2);
         } else {
           cls = 2;
         }
