@@ -47,10 +47,49 @@ WORKLOAD = dict(workload="nside256_10MHz_8sat_1024steps_tilecone1024_mirror513_f
 
 
 def workload_kwargs(prec: str = "fp32_fp64phase") -> dict:
+    """The headline workload (second configuration): bl_max_m = 0 makes the uv
+    grid cover the day's largest |u|, |v| so that every baseline is gridded."""
     import viss_optimize_ws_b200 as vb
     return dict(nside=256, orbit_model=vb.ORBIT_SYNTHETIC, nsat=8, tsteps=1024, segs=4,
                 lambda_m=vb.btag_lambda("10M"), occ_R_m=6371e3, cull="tilecone", viss_tile_pix=1024, mirror=1,
-                grid_res=513, bl_max_m=100e3, orbit_seed=42, precision=prec, occ_mode=2, blockage=1)
+                grid_res=513, bl_max_m=0.0, orbit_seed=42, precision=prec, occ_mode=2, blockage=1)
+
+
+# The five workloads of the metric's definition (synthetic stand-ins with the
+# stated shapes; seeds recorded).  The second is the headline line of main();
+# `--config N` prints a report line for any of them.
+CONFIG_LABELS = {
+    1: "plain method FP64: nside 64, 10 MHz, 8 sats x 64 steps (1,792 half-baselines), 4 segments, "
+       "no tile culling, full grid 256x256",
+    2: "nside 256, 10 MHz, 8 sats x 1,024 steps, 4 segments, tile-cone 1024 + nm1 fast path, mirrored 512x512",
+    3: "precision sweep: nside 512, 30 MHz, 12 sats (66 baselines) x 4,096 steps, 16 segments, tile-cone 4096, "
+       "mirrored 512x512",
+    4: "batched segments: nside 256, 10 MHz, 64 segments of U[50,2000] half-baselines (seed 7), tile-cone 1024, "
+       "mirrored 512x512, autotuned shapes, vs a per-segment launch loop",
+    5: "large sky occ_mode=2: nside 1024, 1 MHz, 16 sats (120 baselines) x 2,048 steps, 128 segments, "
+       "tile-cone 16384, mirrored 1024x1024, FP32 with FP64 phase",
+}
+
+
+def config_kwargs(n: int, prec: str = "fp32_fp64phase") -> dict:
+    import viss_optimize_ws_b200 as vb
+    if n == 2:
+        return workload_kwargs(prec)
+    base = dict(orbit_model=vb.ORBIT_SYNTHETIC, occ_R_m=6371e3, bl_max_m=0.0, orbit_seed=42, precision=prec,
+                occ_mode=2, blockage=1)
+    if n == 1:
+        return dict(base, nside=64, nsat=8, tsteps=64, segs=4, lambda_m=vb.btag_lambda("10M"), cull="none",
+                    mirror=0, grid_res=256)
+    if n == 3:
+        return dict(base, nside=512, nsat=12, tsteps=4096, segs=16, lambda_m=vb.btag_lambda("30M"),
+                    cull="tilecone", viss_tile_pix=4096, mirror=1, grid_res=512)
+    if n == 4:
+        return dict(base, nside=256, nsat=8, segs=64, seg_plan=1, seg_min_half=50, seg_max_half=2000, seg_seed=7,
+                    lambda_m=vb.btag_lambda("10M"), cull="tilecone", viss_tile_pix=1024, mirror=1, grid_res=512)
+    if n == 5:
+        return dict(base, nside=1024, nsat=16, tsteps=2048, segs=128, lambda_m=vb.btag_lambda("1M"),
+                    cull="tilecone", viss_tile_pix=16384, mirror=1, grid_res=1024)
+    raise ValueError(f"no configuration {n}")
 
 
 # ---------------------------------------------------------------------------
@@ -62,6 +101,8 @@ def parse() -> argparse.Namespace:
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 GPU comparison run")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--config", type=int, default=0,
+                    help="print a report line for configuration 1-5 instead of the headline line")
     ap.add_argument("--shape", default="auto",
                     help="kernel shapes: 'auto' (autotuned before the warm-up, untimed), 'default' (built-in), "
                          "or 'bpt,stage_pix,ctas_per_sm,items_per_cta/ppt,items_per_cta' for stage 1 / stage 2")
@@ -187,6 +228,22 @@ def rel_errs(a, b) -> tuple[float, float]:
     return (float(np.abs(d).max() / np.abs(b).max()), float(np.linalg.norm(d) / np.linalg.norm(b)))
 
 
+def err_report(a, b, complex_pairs: bool) -> dict:
+    """Normwise max and RMS relative error of `a` against the reference `b`,
+    and the 99th percentile of the per-element error over the elements with
+    |b| > 1e-3 max |b| (complex magnitudes for interleaved (re, im) pairs)."""
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    if complex_pairs:
+        a = a[0::2] + 1j * a[1::2]
+        b = b[0::2] + 1j * b[1::2]
+    d = np.abs(a - b)
+    mag = np.abs(b)
+    big = mag > 1e-3 * mag.max()
+    return {"max": float(d.max() / mag.max()), "rms": float(np.linalg.norm(d) / np.linalg.norm(mag)),
+            "p99_elem": float(np.percentile(d[big] / mag[big], 99)) if big.any() else 0.0}
+
+
 def traffic_from_profiles(kernel: str) -> float | None:
     """DRAM bytes per launch of `kernel` recorded from an ncu capture in profiles/."""
     for f in sorted((ROOT / "profiles").glob("*.txt")):
@@ -219,6 +276,9 @@ def cpu_sample(stage1_half: int = 64, stage2_pix: int = 1536, seed: int = 1) -> 
     n_half = nbl * T
     # the upstream global horizon is replaced by the Earth horizon at 500 km
     cosphi = float(-np.sqrt(1 - (6371.0 / 6871.0) ** 2))
+    # uv grid covering the day's largest |u|, |v| (as the pipeline's bl_max_m = 0)
+    uvmax = float(max(np.abs(bl["u"]).max(), np.abs(bl["v"]).max()))
+    bl_max = float(np.float32(uvmax * float(lam) * (1.0 + 1e-4)))
     rng = np.random.default_rng(seed)
     ih = np.sort(rng.choice(n_half, stage1_half, replace=False)).astype(np.int32)
     V = np.zeros(2 * stage1_half)
@@ -238,14 +298,14 @@ def cpu_sample(stage1_half: int = 64, stage2_pix: int = 1536, seed: int = 1) -> 
     t0 = time.perf_counter()
     L.or_stage2_subset(npix, P(l), P(m), P(n), nbl, 4, P(seg_t0), P(seg_tl),
                        *[P(bl[k]) for k in ("u", "v", "w", "x1", "y1", "z1", "invn1", "x2", "y2", "z2", "invn2")],
-                       cosphi, P(Vh), 100e3, lam, 513, 0, stage2_pix, P(pix), P(Cout))
+                       cosphi, P(Vh), bl_max, lam, 513, 0, stage2_pix, P(pix), P(Cout))
     t2 = time.perf_counter() - t0
     # groups per segment for the stage-2 term count
     nuniq = 0
     for s in range(4):
         i0, nn = 2 * nbl * seg_t0[s], 2 * nbl * seg_tl[s]
         fa, fb, _ = orp.fa_fb(bl["u"][i0:i0 + nn], bl["v"][i0:i0 + nn], bl["w"][i0:i0 + nn])
-        R, half, du = orp.grid_params(fa, fb, 100e3, lam, 513)
+        R, half, du = orp.grid_params(fa, fb, bl_max, lam, 513)
         k = orp.keys(np.ascontiguousarray(bl["u"][i0:i0 + nn]), np.ascontiguousarray(bl["v"][i0:i0 + nn]), nn // 2,
                      nbl, 1, float(np.float32(1) / np.float32(du)), R, half)
         nuniq += int(np.unique(k).size)
@@ -283,10 +343,177 @@ def run_reference(args) -> None:
 
 
 # ---------------------------------------------------------------------------
+def timed_runs(p, reps: int) -> dict:
+    """`reps` graph replays of both stages (inputs resident); min kernel and
+    stage times in ms and the last report."""
+    r = p.run()
+    best = {"t_s1_kernel_ms": 1e30, "t_s2_kernel_ms": 1e30, "t_stage1_ms": 1e30, "t_stage2_ms": 1e30}
+    for _ in range(reps):
+        r = p.run()
+        for k in best:
+            best[k] = min(best[k], r[k])
+    best["report"] = r
+    best["ms_per_step"] = best["t_stage1_ms"] + best["t_stage2_ms"]
+    best["gterm_s"] = (r["stage1_terms"] + r["stage2_terms"]) / (best["ms_per_step"] * 1e-3) / 1e9
+    return best
+
+
+def per_segment_loop(vb, p, shapes: dict, reps: int) -> dict:
+    """The same day as `p` run segment by segment through the kernel-level C ABI
+    (vb_viss_halfsym, vb_phase_correct_expand, vb_recon_batched with one
+    segment each), as the upstream segment loop launches them; wall time of
+    the whole loop (launch overheads included) and the combined C."""
+    L = vb.lib()
+    from viss_optimize_ws_b200._lib import DeviceBuffer
+    cfg = p.cfg
+    sky = vb.Sky()
+    sky.npix = p.npix
+    for k in ("B", "l", "m", "n", "cx", "cy", "cz", "cosA", "sinA"):
+        setattr(sky, k, p.ptr(k)[0])
+    sky.tile_pix = cfg.viss_tile_pix
+    t0s, tls = p.seg_plan()
+    nbl = p.nbl
+    rep = p.run()
+    o1 = vb.Stage1Opts(precision=cfg.precision, cull=cfg.cull, phase_corrected=1, blockage=cfg.blockage,
+                       bpt=shapes.get("stage1_bpt", 0), stage_pix=shapes.get("stage1_stage_pix", 0),
+                       ctas_per_sm=shapes.get("stage1_ctas_per_sm", 0), items_per_cta=shapes.get("stage1_items_per_cta", 0))
+    o2 = vb.Stage2Opts(mirror=cfg.mirror, blockage=cfg.blockage, occ_mode=cfg.occ_mode, precision=cfg.precision,
+                       cull=cfg.stage2_cull, grid_res=cfg.grid_res, bl_max=rep["bl_max_m"], lambda_=cfg.lambda_m,
+                       ppt=shapes.get("stage2_ppt", 0), items_per_cta=shapes.get("stage2_items_per_cta", 0))
+    keys = ("u", "v", "w", "x1", "y1", "z1", "x2", "y2", "z2", "invn1", "invn2", "cosphi1", "cosphi2")
+    base = {k: p.ptr(k)[0] for k in keys}
+    segs = []
+    for t0, tl in zip(t0s, tls):
+        b = vb.Baselines()
+        b.n_full, b.nbl, b.cosphi = 2 * nbl * int(tl), nbl, p.cosphi
+        off = 4 * 2 * nbl * int(t0)
+        for k in keys:
+            if base[k]:
+                setattr(b, k, base[k] + off)
+        segs.append(b)
+    need1 = max(L.vb_stage1_workspace_bytes(C.byref(sky), C.byref(b), C.byref(o1)) for b in segs)
+    need2 = max(L.vb_stage2_workspace_bytes(b.n_full // 2, 1, p.npix, C.byref(o2)) for b in segs)
+    nh_max = max(b.n_full // 2 for b in segs)
+    ws1, ws2 = DeviceBuffer(need1), DeviceBuffer(need2)
+    Vd, Vh = DeviceBuffer(16 * nh_max), DeviceBuffer(8 * nh_max)
+    Cs = [DeviceBuffer(4 * p.npix) for _ in segs]
+    Ws = [DeviceBuffer(4 * p.npix) for _ in segs]
+    st0 = DeviceBuffer(4)
+    vb.check(L.vb_memset(st0.ptr, 0, 4))
+    stl = []
+    for tl in tls:
+        d = DeviceBuffer(4)
+        h = np.array([tl], np.int32)
+        vb.check(L.vb_memcpy(d.ptr, h.ctypes.data, 4, 0))
+        stl.append(d)
+    best = 1e30
+    for _ in range(reps + 1):
+        vb.check(L.vb_synchronize())
+        t = time.perf_counter()
+        for i, b in enumerate(segs):
+            vb.check(L.vb_viss_halfsym(C.byref(sky), C.byref(b), C.byref(o1), ws1.ptr, need1, Vd.ptr, None, None))
+            vb.check(L.vb_phase_correct_expand(Vd.ptr, b.w, b.n_full // 2, nbl, 1, Vh.ptr, None, None))
+            vb.check(L.vb_recon_batched(C.byref(sky), C.byref(b), Vh.ptr, 1, st0.ptr, stl[i].ptr, C.byref(o2),
+                                        ws2.ptr, need2, Cs[i].ptr, Ws[i].ptr, None, None, None))
+        vb.check(L.vb_synchronize())
+        best = min(best, time.perf_counter() - t)
+    num = np.zeros(p.npix)
+    den = np.zeros(p.npix)
+    for c, w in zip(Cs, Ws):
+        cc, ww = c.to_array(np.float32).astype(np.float64), w.to_array(np.uint32).astype(np.float64)
+        num += cc * ww
+        den += ww
+    Cloop = np.where(den > 0, num / np.maximum(den, 1), 0.0)
+    return {"ms_per_step": best * 1e3, "launch_calls": 3 * len(segs), "C": Cloop}
+
+
+def run_config_report(args) -> None:
+    """One JSON report line for configuration `args.config` (throughput,
+    errors against the FP64 build, and the configuration's own comparisons)."""
+    import viss_optimize_ws_b200 as vb
+    n = args.config
+    vb.check(vb.lib().vb_set_device(0))
+    sfu, f32, f64, clk = (C.c_double() for _ in range(4))
+    vb.check(vb.lib().vb_measure_peaks(C.byref(sfu), C.byref(f32), C.byref(f64), C.byref(clk)))
+    peak = sfu.value / 1e9   # G sin+cos pairs / s
+    kw = config_kwargs(n)
+    B = vb.synthetic_sky(kw["nside"], seed=1)
+    reps = 3 if n in (3, 5) else 5
+    out = {"impl": "b200", "report": f"config {n}", "label": CONFIG_LABELS[n], "unit": UNIT, "data": "synthetic",
+           "sky": "U[0,1) + 20 point sources x 10, seed 1", "orbit_seed": 42,
+           "sfu_peak_g_pairs_s": peak, "sm_clock_mhz_microbench": clk.value}
+    # FP64 build: the reference for every error below
+    q = vb.Pipeline(vb.run_config(**config_kwargs(n, "fp64")))
+    q.set_sky(B)
+    q.make_baselines()
+    t64 = timed_runs(q, 1 if n in (3, 5) else 2)
+    V64, C64, W64 = q.get("V_half"), q.get("C"), q.get("W")
+    r64 = t64["report"]
+    uvw = [float(np.abs(q.get(k)).max()) for k in ("u", "v", "w")]
+    out["sizes"] = {"npix": r64["npix"], "n_half": r64["n_half_total"], "nseg": r64["nseg"],
+                    "groups": r64["groups_total"], "stage1_terms": r64["stage1_terms"],
+                    "stage2_terms": r64["stage2_terms"], "max_abs_uvw": uvw, "bl_max_m": r64["bl_max_m"]}
+    out["fp64_gpu"] = {"ms_per_step": t64["ms_per_step"], "gterm_s": t64["gterm_s"]}
+    precs = ["fp32_fp64phase", "fp32_dsphase", "ref32"] if n == 3 else ["fp32_fp64phase"]
+    out["mixed"] = {}
+    shapes = {}
+    for prec in precs:
+        p = vb.Pipeline(vb.run_config(**config_kwargs(n, prec)))
+        p.set_sky(B)
+        p.make_baselines()
+        tune = p.autotune(reps=2) if (n in (1, 2, 4) and prec == "fp32_fp64phase") else None
+        if tune:
+            shapes = tune
+        t = timed_runs(p, reps)
+        r = t["report"]
+        ev = err_report(p.get("V_half"), V64, True)
+        ec = err_report(p.get("C"), C64, False)
+        out["mixed"][prec] = {
+            "ms_per_step": t["ms_per_step"], "gterm_s": t["gterm_s"], "speedup_vs_fp64": t64["ms_per_step"] / t["ms_per_step"],
+            "stage1_kernel_ms": t["t_s1_kernel_ms"], "stage2_kernel_ms": t["t_s2_kernel_ms"],
+            "stage1_eval_terms": int(r["s1_counters"][0] + r["s1_counters"][1]),
+            "stage2_eval_terms": int(r["s2_counters"][0] + r["s2_counters"][1]),
+            "stage1_sfu_frac": (r["s1_counters"][0] + r["s1_counters"][1]) / (t["t_s1_kernel_ms"] * 1e-3) / 1e9 / peak,
+            "stage2_sfu_frac": (r["s2_counters"][0] + r["s2_counters"][1]) / (t["t_s2_kernel_ms"] * 1e-3) / 1e9 / peak,
+            "err_V": ev, "err_C": ec, "W_equal_fp64": bool(np.array_equal(p.get("W"), W64)),
+            "error_flags": r["error_flags"], "autotune": tune}
+        if prec == "fp32_fp64phase" and n == 4:
+            loop = per_segment_loop(vb, p, shapes, 2)
+            out["per_segment_loop"] = {"ms_per_step": loop["ms_per_step"], "launch_calls": loop["launch_calls"],
+                                       "batched_graph_ms_per_step": t["ms_per_step"],
+                                       "speedup_batched": loop["ms_per_step"] / t["ms_per_step"],
+                                       "C_vs_batched": err_report(loop["C"], p.get("C"), False)}
+        p.close()
+    if n == 1:
+        # the plain method on the host cores: the oracle's FP64 restatement, whole day
+        from oracle import py as orp
+        sky = {k: q.get(k) for k in ("B", "l", "m", "n")}
+        bl = {k: q.get(k) for k in ("u", "v", "w", "x1", "y1", "z1", "x2", "y2", "z2", "invn1", "invn2", "cosphi1",
+                                    "cosphi2")}
+        bl = {k: v for k, v in bl.items() if v.size}
+        bl["nbl"], bl["cosphi"] = q.nbl, q.cosphi
+        t0s, tls = q.seg_plan()
+        tc = time.perf_counter()
+        Vc = orp.stage1(sky, bl, phase_corrected=1, precision=1)
+        Cc, Wc, _ = orp.stage2(sky, bl, Vc.astype(np.float32), t0s, tls, mirror=0, blockage=1, occ_mode=2,
+                               bl_max=r64["bl_max_m"], lam=float(q.cfg.lambda_m), grid_res=256, precision=1)
+        tcpu = time.perf_counter() - tc
+        out["cpu_fp64_oracle"] = {"ms_per_step": tcpu * 1e3, "cores": orp.oracle().or_num_threads(),
+                                  "gterm_s": (r64["stage1_terms"] + r64["stage2_terms"]) / tcpu / 1e9,
+                                  "gpu_fp64_vs_cpu_V": err_report(V64, Vc, True),
+                                  "gpu_fp64_vs_cpu_C": err_report(C64, Cc, False),
+                                  "W_equal": bool(np.array_equal(W64, Wc))}
+    q.close()
+    print(json.dumps(out), flush=True)
+
+
 def main() -> None:
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+        return
+    if args.config:
+        run_config_report(args)
         return
     import viss_optimize_ws_b200 as vb
     ws, rank, local = dist_env()

@@ -328,7 +328,7 @@ typedef struct {
   double   dt_s;
   double   alt_min_km, alt_max_km, spread_km;
   double   occ_R_m;        /* <= 0: upstream global cosphi from R=1737.1 km, h=300 km */
-  float    bl_max_m;       /* upstream 100e3 */
+  float    bl_max_m;       /* upstream 100e3; <= 0: the uv grid covers the day's largest |u|, |v| */
   int      grid_res;       /* > 0 forces RES */
   int      seg_plan;       /* 0: even split (upstream); 1: seeded uneven counts */
   int      seg_min_half, seg_max_half;  /* seg_plan=1: half-baseline count range per segment */
@@ -363,6 +363,7 @@ typedef struct {
   double   t_e2e_ms;       /* vb_pipeline_run_host: H2D, baselines, both stages, D2H */
   int      error_flags;    /* device-side error word (0 = ok) */
   int      graph_kernels;  /* kernel nodes of the captured run graph (0 = eager) */
+  double   bl_max_m;       /* bl_max the uv grids were built with (the automatic value when bl_max_m <= 0) */
 } vb_report;
 
 void vb_run_config_defaults(vb_run_config* c);

@@ -84,7 +84,8 @@ class Report(C.Structure):
                 ("t_stage1_ms", C.c_double), ("t_stage2_ms", C.c_double), ("t_orbit_ms", C.c_double),
                 ("s1_counters", C.c_ulonglong * 4), ("s2_counters", C.c_ulonglong * 4),
                 ("w_scalar_total", C.c_double), ("t_s1_kernel_ms", C.c_double), ("t_s2_kernel_ms", C.c_double),
-                ("t_e2e_ms", C.c_double), ("error_flags", C.c_int), ("graph_kernels", C.c_int)]
+                ("t_e2e_ms", C.c_double), ("error_flags", C.c_int), ("graph_kernels", C.c_int),
+                ("bl_max_m", C.c_double)]
 
     def as_dict(self) -> dict:
         d = {k: getattr(self, k) for k, _ in self._fields_ if k not in ("s1_counters", "s2_counters")}

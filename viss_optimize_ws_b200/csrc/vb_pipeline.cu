@@ -101,6 +101,8 @@ struct vb_pipeline {
   float *x2 = nullptr, *y2 = nullptr, *z2 = nullptr, *in1 = nullptr, *in2 = nullptr, *cp1 = nullptr,
         *cp2 = nullptr;
   bool baselines_ready = false;
+  float auto_bl_max = 0.f;       // bl_max_m <= 0: measured by make_baselines
+  unsigned* d_uvmax = nullptr;   // scratch of that measurement
   // stage 1
   Stage1Plan p1{};
   void* ws1 = nullptr;
@@ -437,9 +439,43 @@ static int make_baselines_async(vb_pipeline* p) {
   return VB_OK;
 }
 
+// max(|u|, |v|) over n values; out is one uint holding the float's bits
+// (non-negative floats order as their bit patterns).
+__global__ void k_uv_absmax(const float* __restrict__ u, const float* __restrict__ v, int n, unsigned* out) {
+  float mx = 0.f;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    mx = fmaxf(mx, fmaxf(fabsf(u[i]), fabsf(v[i])));
+  for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  if ((threadIdx.x & 31) == 0 && mx == mx) atomicMax(out, __float_as_uint(mx));
+}
+
+// bl_max_m <= 0: grid half-width = the largest |u|, |v| of the day's
+// baselines (wavelengths -> metres); synchronises.
+static int measure_bl_max(vb_pipeline* p) {
+  if (!p->d_uvmax) VB_TRY(dalloc(p, &p->d_uvmax, 1));
+  VB_CUDA(cudaMemsetAsync(p->d_uvmax, 0, sizeof(unsigned), p->s));
+  int g = (int)std::min<int64_t>(ceil_div(p->n_full, 256), (int64_t)sm_count() * 8);
+  k_uv_absmax<<<g > 0 ? g : 1, 256, 0, p->s>>>(p->u, p->v, p->n_full, p->d_uvmax);
+  VB_LAUNCH_CHECK();
+  unsigned bits = 0;
+  VB_CUDA(cudaMemcpyAsync(&bits, p->d_uvmax, sizeof(unsigned), cudaMemcpyDeviceToHost, p->s));
+  VB_CUDA(cudaStreamSynchronize(p->s));
+  float mx = 0.f;
+  std::memcpy(&mx, &bits, sizeof(mx));
+  const float bl = (float)((double)mx * (double)p->cfg.lambda_m * (1.0 + 1e-4));
+  if (!(bl > 0.f)) return fail(VB_ERR_INVALID, "automatic bl_max: the baselines have no extent");
+  if (bl != p->auto_bl_max) {
+    p->auto_bl_max = bl;
+    p->p2.bl_max = bl;
+    drop_graph(p);
+  }
+  return VB_OK;
+}
+
 extern "C" int vb_pipeline_make_baselines(vb_pipeline* p) {
   if (!p) return fail(VB_ERR_INVALID, "vb_pipeline_make_baselines: null pipeline");
   VB_TRY(make_baselines_async(p));
+  if (p->cfg.bl_max_m <= 0.f) VB_TRY(measure_bl_max(p));
   int bad = -1;
   VB_TRY(vb_validate_uvw_halfsym(p->u, p->v, p->w, p->n_full, p->nbl, &bad, p->s));
   p->baselines_ready = true;
@@ -464,6 +500,14 @@ static int enqueue_stages(vb_pipeline* p) {
                     p->segp, p->counters + 4, p->wsum, p->s, &pre, p->ev[7], p->ev[8]));
   VB_CUDA(record_event(p->ev[2], p->s));
   return VB_OK;
+}
+
+// bl_max of the uv grids: the configured value, or (bl_max_m <= 0) the day's
+// largest |u|, |v| in metres with a 1e-4 margin, measured by make_baselines
+// (a placeholder of 1 m until then).
+static float effective_bl_max(const vb_pipeline* p) {
+  if (p->cfg.bl_max_m > 0.f) return p->cfg.bl_max_m;
+  return p->auto_bl_max > 0.f ? p->auto_bl_max : 1.0f;
 }
 
 // Stage plans from the run config (kernel shapes included), workspaces grown
@@ -493,7 +537,7 @@ static int plan_stages(vb_pipeline* p) {
   o2.ppt = c->stage2_ppt;
   o2.items_per_cta = c->stage2_items_per_cta;
   o2.grid_res = c->grid_res;
-  o2.bl_max = c->bl_max_m;
+  o2.bl_max = effective_bl_max(p);
   o2.lambda = c->lambda_m;
   Stage2Plan p2;
   VB_TRY(stage2_plan(p->n_half, p->nseg, p->npix, &o2, &p2));
@@ -527,6 +571,7 @@ static int fill_report(vb_pipeline* p, vb_report* r) {
   r->t_s1_kernel_ms = k1;
   r->t_s2_kernel_ms = k2;
   r->graph_kernels = p->graph_kernels;
+  r->bl_max_m = effective_bl_max(p);
   unsigned long long cnt[8];
   VB_CUDA(cudaMemcpy(cnt, p->counters, sizeof(cnt), cudaMemcpyDeviceToHost));
   for (int k = 0; k < 4; ++k) {
@@ -618,6 +663,7 @@ extern "C" int vb_pipeline_run_host(vb_pipeline* p, const float* B_host, int sca
   VB_CUDA(record_event(p->ev[3], p->s));
   VB_TRY(set_sky_async(p, B_host, scale));
   VB_TRY(make_baselines_async(p));
+  if (p->cfg.bl_max_m <= 0.f && !(p->auto_bl_max > 0.f)) VB_TRY(measure_bl_max(p));   // first call only
   p->baselines_ready = true;
   vb_sky sky = sky_of(p);
   VB_TRY(stage1_prepare_pixels(&sky, p->p1, p->b1, p->s));
