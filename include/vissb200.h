@@ -403,6 +403,18 @@ int vb_pipeline_seg_plan(vb_pipeline* p, int* seg_t0, int* seg_tlen);   /* host 
 int vb_pipeline_seg_params(vb_pipeline* p, vb_seg_params* host_out);     /* host array of nseg; syncs */
 int vb_pipeline_destroy(vb_pipeline* p);
 
+/* Switches the pipeline to another day of the same run (new orbit window /
+ * formation draw for that day, same buffers, plans and captured graph); the
+ * next run generates the day's baselines.  Fails if the day's orbit has a
+ * different step or pair count.  Replaces the per-day re-initialisation of
+ * the upstream day loop (main_recon_online_mirror_tile_vissfast.cu:274-290). */
+int vb_pipeline_set_day(vb_pipeline* p, int day);
+
+/* acc[i] += C[i] in FP64 on the device (n values): the cross-day running sum
+ * of daily images that the upstream post-processing keeps in a file
+ * (combine.py:42-126, mirror_tile_vissfast/viss_monitor.py:92-139). */
+int vb_accumulate(const float* C, int64_t n, double* acc, void* stream);
+
 /* Autotuner (no upstream counterpart: upstream fixes 256-thread blocks and one
  * block per 256 baselines or pixels).  Times the stage-1 kernel over baselines
  * per thread x staged pixels x resident CTAs per SM x work-queue granularity,

@@ -118,3 +118,36 @@ def test_parameter_scripts_and_autotune(gpu, vb, tmp_path):
                        env=env, capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
     assert (tmp_path / "root" / "C1day1M.txt").exists() and (tmp_path / "root" / "Viss1day1M.txt").exists()
+
+
+def test_multi_day_running_sum_and_resume(gpu, vb, tmp_path):
+    """--day_count > 1 reuses one run context (vb_pipeline_set_day); the
+    --accum_file running sum equals the sum of the daily images and resumes
+    from its file like the upstream accumulator daemon (viss_monitor.py)."""
+    exe = BIN / "main_recon_online_mirror_tile_vissfast"
+    sky = tmp_path / "sky"
+    common = ["--btag=1M", "--nside=16", "--segs=2", "--blockage=1", "--occ_mode=2", f"--sky_dir={sky}", "--gpus=0",
+              "--B_mode=bin", "--C_mode=bin", "--orbit_seed=42", "--sky_gen=3"]
+    a, b, c = tmp_path / "a", tmp_path / "b", tmp_path / "c"
+    r = run(exe, common + ["--day_start=1", "--day_count=3", f"--out_dir={a}/", f"--accum_file={a}/sum.bin"], tmp_path)
+    assert r.returncode == 0, r.stderr
+    daily = [np.fromfile(a / f"C{d}day1M.bin", dtype=np.float32) for d in (1, 2, 3)]
+    acc = np.fromfile(a / "sum.bin", dtype=np.float32)
+    ref = np.sum([d.astype(np.float64) for d in daily], axis=0)
+    assert np.abs(acc - ref).max() <= 1e-6 * np.abs(ref).max()
+    log = (a / "sum.bin.log").read_text().splitlines()
+    assert len(log) == 3 and [ln.split(" | ")[1] for ln in log] == ["C1", "C2", "C3"]
+    # a later day in its own process equals the same day of the multi-day run
+    r = run(exe, common + ["--day_start=3", "--day_count=1", f"--out_dir={b}/"], tmp_path)
+    assert r.returncode == 0, r.stderr
+    assert np.array_equal(np.fromfile(b / "C3day1M.bin", dtype=np.float32).view(np.uint32), daily[2].view(np.uint32))
+    # resume: days 1-2, then day 3 from the saved sum, daily files not kept
+    r = run(exe, common + ["--day_start=1", "--day_count=2", f"--out_dir={c}/", f"--accum_file={c}/sum.bin"], tmp_path)
+    assert r.returncode == 0, r.stderr
+    r = run(exe, common + ["--day_start=3", "--day_count=1", f"--out_dir={c}/", f"--accum_file={c}/sum.bin",
+                           "--keep_daily=0"], tmp_path)
+    assert r.returncode == 0, r.stderr
+    assert "Resuming running sum" in r.stdout
+    assert not (c / "C3day1M.bin").exists()
+    acc2 = np.fromfile(c / "sum.bin", dtype=np.float32)
+    assert np.abs(acc2 - acc).max() <= 1e-6 * np.abs(ref).max()

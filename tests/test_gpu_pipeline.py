@@ -166,3 +166,45 @@ def test_autotune_keeps_results_and_picks_a_valid_shape(gpu, vb):
         # a second run of the tuned graph is bit-identical
         p.run()
         assert np.array_equal(p.get("C").view(np.uint32), C1.view(np.uint32))
+
+
+def test_set_day_matches_a_fresh_pipeline(gpu, vb):
+    """vb_pipeline_set_day swaps the day's orbit in a live pipeline (buffers,
+    plans and graph kept): results are bit-identical to a pipeline created for
+    that day; a day with another step count is refused."""
+    kw = dict(nside=16, orbit_model=vb.ORBIT_REFERENCE, segs=2, lambda_m=vb.btag_lambda("1M"), mirror=1,
+              cull="tilecone", viss_tile_pix=256, grid_res=0, bl_max_m=0.0)
+    B = vb.synthetic_sky(16, seed=5)
+    with vb.Pipeline(vb.run_config(day=1, **kw)) as p:
+        p.set_sky(B)
+        p.make_baselines()
+        p.run()
+        vb.check(vb.lib().vb_pipeline_set_day(p.h, 2))
+        r = p.run()
+        assert r["error_flags"] == 0
+        C2, V2 = p.get("C"), p.get("V_half")
+    with vb.Pipeline(vb.run_config(day=2, **kw)) as q:
+        q.set_sky(B)
+        q.make_baselines()
+        q.run()
+        assert np.array_equal(q.get("C").view(np.uint32), C2.view(np.uint32))
+        assert np.array_equal(q.get("V_half").view(np.uint32), V2.view(np.uint32))
+    # synthetic model: tsteps fixed by the config, so any day keeps the shape
+    with vb.Pipeline(vb.run_config(nside=8, orbit_model=vb.ORBIT_SYNTHETIC, nsat=4, tsteps=8, segs=2,
+                                   lambda_m=30.0, occ_R_m=6371e3, grid_res=33)) as s:
+        s.set_sky(vb.synthetic_sky(8))
+        s.make_baselines()
+        vb.check(vb.lib().vb_pipeline_set_day(s.h, 7))
+        s.run()
+
+
+def test_device_accumulate(gpu, vb):
+    from gpu_util import dev, get, zeros
+    rng = np.random.default_rng(2)
+    a = rng.standard_normal(5000).astype(np.float32)
+    acc = zeros(5000, np.float64)
+    da = dev(a)
+    for _ in range(3):
+        vb.check(vb.lib().vb_accumulate(da.ptr, a.size, acc.ptr, None))
+    vb.check(vb.lib().vb_synchronize())
+    assert np.array_equal(get(acc, np.float64), 3 * a.astype(np.float64))

@@ -156,6 +156,8 @@ _SIGS = {
     "vb_pipeline_seg_params": (C.c_int, [vp, vp]),
     "vb_pipeline_destroy": (C.c_int, [vp]),
     "vb_pipeline_autotune": (C.c_int, [vp, C.c_int, C.POINTER(TuneReport)]),
+    "vb_pipeline_set_day": (C.c_int, [vp, C.c_int]),
+    "vb_accumulate": (C.c_int, [vp, C.c_int64, vp, vp]),
     "vb_abi_sizeof": (C.c_size_t, [C.c_char_p]),
     "vb_measure_peaks": (C.c_int, [C.POINTER(C.c_double)] * 4),
     "vb_flush_l2": (C.c_int, [vp, C.c_size_t, vp]),

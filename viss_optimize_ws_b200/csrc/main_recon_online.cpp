@@ -18,6 +18,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <ctime>
 #include <fstream>
 #include <iomanip>
 #include <iostream>
@@ -188,6 +189,10 @@ int main(int argc, char** argv) {
   std::string report_json = get_arg(argc, argv, "--report_json", "");
   int stage2_cull = to_int(get_arg(argc, argv, "--stage2_cull", "2"), 2);
   int autotune = to_int(get_arg(argc, argv, "--autotune", "0"), 0);
+  // cross-day running sum of the daily C (the upstream accumulator daemon,
+  // viss_monitor.py / combine.py), kept on the device in FP64
+  std::string accum_file = get_arg(argc, argv, "--accum_file", "");
+  int keep_daily = to_int(get_arg(argc, argv, "--keep_daily", "1"), 1);
 
   if (btag != "1M" && btag != "10M" && btag != "30M") return die("ERROR --btag");
   if (nside <= 0) nside = (btag == "1M") ? 512 : (btag == "10M" ? 4096 : 16384);
@@ -284,15 +289,40 @@ int main(int argc, char** argv) {
 
   std::ostringstream json;
   json << "{\"days\": [";
+  // one run context for all days: each further day only swaps the orbit
+  vb_pipeline* p = nullptr;
+  double* d_acc = nullptr;
   for (int di = 0; di < day_count; ++di) {
     const int dayid = day_start + di;
     cfg.day = dayid;
     if (vissfast) std::cout << "===== Day " << dayid << " / " << (day_start + day_count - 1) << " =====\n";
     Timer t_init;
     t_init.tic();
-    vb_pipeline* p = nullptr;
-    if (vb_pipeline_create(&cfg, &p) != VB_OK) return die(std::string("ERROR ") + vb_last_error());
-    if (vb_pipeline_set_sky(p, hB.data(), 1) != VB_OK) return die(std::string("ERROR ") + vb_last_error());
+    if (!p) {
+      if (vb_pipeline_create(&cfg, &p) != VB_OK) return die(std::string("ERROR ") + vb_last_error());
+      if (vb_pipeline_set_sky(p, hB.data(), 1) != VB_OK) return die(std::string("ERROR ") + vb_last_error());
+      if (!accum_file.empty()) {
+        // resume from an existing running sum (float32, npix) or start at zero
+        if (vb_malloc(reinterpret_cast<void**>(&d_acc), (size_t)npix * sizeof(double)) != VB_OK)
+          return die(std::string("ERROR ") + vb_last_error());
+        std::vector<double> a((size_t)npix, 0.0);
+        std::ifstream in(accum_file, std::ios::binary | std::ios::ate);
+        if (in.is_open()) {
+          if ((int64_t)in.tellg() != npix * (int64_t)sizeof(float))
+            return die("ERROR accum_file " + accum_file + " does not hold npix float32 values");
+          in.seekg(0);
+          std::vector<float> f((size_t)npix);
+          in.read(reinterpret_cast<char*>(f.data()), (std::streamsize)(npix * sizeof(float)));
+          if (!in) return die("ERROR reading " + accum_file);
+          for (int64_t i = 0; i < npix; ++i) a[i] = f[i];
+          std::cout << "Resuming running sum from " << accum_file << "\n";
+        }
+        if (vb_memcpy(d_acc, a.data(), a.size() * sizeof(double), VB_H2D) != VB_OK)
+          return die(std::string("ERROR ") + vb_last_error());
+      }
+    } else if (vb_pipeline_set_day(p, dayid) != VB_OK) {
+      return die(std::string("ERROR ") + vb_last_error());
+    }
     int64_t np_ = 0;
     int nseg = 0, n_half = 0, nbl = 0, ntile = 0;
     float cp = 0;
@@ -415,7 +445,43 @@ int main(int argc, char** argv) {
     std::vector<float> Cout = dv.get("C");
     const bool txt = (C_mode == "txt");
     std::string outC = out_dir + "C" + dtag + (txt ? ".txt" : ".bin");
-    if (txt) {
+    if (d_acc) {
+      // running sum: device FP64 += C, file = float32 sum, log line per day
+      Timer t_a;
+      t_a.tic();
+      void* dC = nullptr;
+      int64_t nC = 0;
+      if (vb_pipeline_device_ptr(p, "C", &dC, &nC) != VB_OK ||
+          vb_accumulate(static_cast<const float*>(dC), nC, d_acc, nullptr) != VB_OK || vb_synchronize() != VB_OK)
+        return die(std::string("ERROR ") + vb_last_error());
+      std::vector<double> a((size_t)npix);
+      if (vb_memcpy(a.data(), d_acc, a.size() * sizeof(double), VB_D2H) != VB_OK)
+        return die(std::string("ERROR ") + vb_last_error());
+      std::vector<float> f((size_t)npix);
+      double mean = 0.0, mn = INFINITY, mx = -INFINITY;
+      for (int64_t i = 0; i < npix; ++i) {
+        f[i] = (float)a[i];
+        mean += a[i];
+        mn = std::min(mn, a[i]);
+        mx = std::max(mx, a[i]);
+      }
+      mean /= (double)npix;
+      std::ofstream o(accum_file, std::ios::binary | std::ios::trunc);
+      o.write(reinterpret_cast<const char*>(f.data()), (std::streamsize)(npix * sizeof(float)));
+      if (!o) return die("ERROR writing " + accum_file);
+      o.close();
+      std::time_t now = std::time(nullptr);
+      char ts[32];
+      std::strftime(ts, sizeof(ts), "%Y-%m-%d %H:%M:%S", std::localtime(&now));
+      std::ofstream lg(accum_file + ".log", std::ios::app);
+      lg << ts << " | C" << dayid << " | time=" << std::fixed << std::setprecision(1) << t_a.toc_s()
+         << "s | mean=" << std::setprecision(6) << mean << "\n";
+      std::cout << "Accumulated day " << dayid << " into " << accum_file << ": mean=" << mean << " min=" << mn
+                << " max=" << mx << "\n";
+    }
+    if (!keep_daily) {
+      std::cout << "Daily C not written (--keep_daily=0)\n";
+    } else if (txt) {
       std::ofstream ofs(outC);
       if (!ofs.is_open()) return die("ERROR open " + outC);
       std::vector<char> buf(8 << 20);
@@ -426,13 +492,14 @@ int main(int argc, char** argv) {
       if (!ofs.is_open()) return die("ERROR open " + outC);
       ofs.write(reinterpret_cast<const char*>(Cout.data()), (std::streamsize)(Cout.size() * sizeof(float)));
     }
-    std::cout << "Wrote " << outC << " in " << t_w.toc_s() << " s\n";
+    if (keep_daily) std::cout << "Wrote " << outC << " in " << t_w.toc_s() << " s\n";
     json << (di ? ", " : "") << "{\"day\": " << dayid << ", \"t_stage1_ms\": " << rep.t_stage1_ms
          << ", \"t_stage2_ms\": " << rep.t_stage2_ms << ", \"stage1_terms\": " << rep.stage1_terms
          << ", \"stage2_terms\": " << rep.stage2_terms << ", \"groups\": " << rep.groups_total
          << ", \"error_flags\": " << rep.error_flags << "}";
-    vb_pipeline_destroy(p);
   }
+  if (p) vb_pipeline_destroy(p);
+  if (d_acc) vb_free(d_acc);
   json << "]}";
   if (!report_json.empty()) {
     std::ofstream o(report_json);

@@ -285,6 +285,25 @@ static int uneven_total_steps(const vb_run_config& c, int nbl) {
 
 static int plan_stages(vb_pipeline* p);
 
+static vb_orbit_params orbit_params_of(const vb_run_config& c) {
+  vb_orbit_params op{};
+  op.model = c.orbit_model;
+  op.lambda_m = c.lambda_m;
+  op.day = c.day;
+  op.seed = c.orbit_seed;
+  op.nsat = c.orbit_model == VB_ORBIT_REFERENCE ? 8 : c.nsat;
+  op.dt_s = c.dt_s;
+  op.alt_min_km = c.alt_min_km;
+  op.alt_max_km = c.alt_max_km;
+  op.spread_km = c.spread_km;
+  op.occ_R_m = c.occ_R_m;
+  if (c.orbit_model == VB_ORBIT_SYNTHETIC) {
+    int nbl = op.nsat * (op.nsat - 1) / 2;
+    op.tsteps = (c.seg_plan == 1) ? uneven_total_steps(c, nbl) : c.tsteps;
+  }
+  return op;
+}
+
 extern "C" int vb_pipeline_create(const vb_run_config* c, vb_pipeline** out) {
   if (!c || !out) return fail(VB_ERR_INVALID, "vb_pipeline_create: null argument");
   *out = nullptr;
@@ -349,21 +368,7 @@ extern "C" int vb_pipeline_create(const vb_run_config* c, vb_pipeline** out) {
   }
 
   // orbit generator
-  vb_orbit_params op{};
-  op.model = c->orbit_model;
-  op.lambda_m = c->lambda_m;
-  op.day = c->day;
-  op.seed = c->orbit_seed;
-  op.nsat = c->orbit_model == VB_ORBIT_REFERENCE ? 8 : c->nsat;
-  op.dt_s = c->dt_s;
-  op.alt_min_km = c->alt_min_km;
-  op.alt_max_km = c->alt_max_km;
-  op.spread_km = c->spread_km;
-  op.occ_R_m = c->occ_R_m;
-  if (c->orbit_model == VB_ORBIT_SYNTHETIC) {
-    int nbl = op.nsat * (op.nsat - 1) / 2;
-    op.tsteps = (c->seg_plan == 1) ? uneven_total_steps(*c, nbl) : c->tsteps;
-  }
+  vb_orbit_params op = orbit_params_of(*c);
   PTRY(vb_orbit_create(&op, &p->orb));
   PTRY(vb_orbit_info(p->orb, &p->T, &p->nbl, nullptr, nullptr, nullptr));
   PTRY(make_seg_plan(*c, p->T, p->nbl, c->orbit_model == VB_ORBIT_SYNTHETIC, p->h_t0, p->h_tlen));
@@ -836,6 +841,46 @@ extern "C" size_t vb_abi_sizeof(const char* name) {
   for (const Entry& e : table)
     if (std::strcmp(e.n, name) == 0) return e.s;
   return 0;
+}
+
+extern "C" int vb_pipeline_set_day(vb_pipeline* p, int day) {
+  if (!p) return fail(VB_ERR_INVALID, "vb_pipeline_set_day: null pipeline");
+  VB_CUDA(cudaSetDevice(p->cfg.device));
+  if (day == p->cfg.day) return VB_OK;
+  vb_run_config c = p->cfg;
+  c.day = day;
+  vb_orbit_params op = orbit_params_of(c);
+  vb_orbit* o = nullptr;
+  VB_CUDA(cudaStreamSynchronize(p->s));
+  VB_TRY(vb_orbit_create(&op, &o));
+  int T = 0, nbl = 0;
+  int rc = vb_orbit_info(o, &T, &nbl, nullptr, nullptr, nullptr);
+  if (rc == VB_OK && (T != p->T || nbl != p->nbl))
+    rc = fail(VB_ERR_UNSUPPORTED, "vb_pipeline_set_day: day %d has %d steps x %d pairs, the pipeline %d x %d", day, T,
+              nbl, p->T, p->nbl);
+  if (rc != VB_OK) {
+    vb_orbit_destroy(o);
+    return rc;
+  }
+  vb_orbit_destroy(p->orb);
+  p->orb = o;
+  p->cfg.day = day;
+  p->baselines_ready = false;
+  return VB_OK;
+}
+
+__global__ void k_accumulate(const float* __restrict__ C, int64_t n, double* __restrict__ acc) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    acc[i] += (double)C[i];
+}
+
+extern "C" int vb_accumulate(const float* C, int64_t n, double* acc, void* stream) {
+  if (n < 0 || (n > 0 && (!C || !acc))) return fail(VB_ERR_INVALID, "vb_accumulate: bad arguments");
+  if (n == 0) return VB_OK;
+  int g = (int)std::min<int64_t>(ceil_div(n, 256), (int64_t)sm_count() * 16);
+  k_accumulate<<<g, 256, 0, as_stream(stream)>>>(C, n, acc);
+  VB_LAUNCH_CHECK();
+  return VB_OK;
 }
 
 extern "C" int vb_pipeline_destroy(vb_pipeline* p) {
