@@ -340,6 +340,9 @@ typedef struct {
   int      stage1_stage_pix;      /* vb_stage1_opts.stage_pix */
   int      stage1_ctas_per_sm;    /* vb_stage1_opts.ctas_per_sm */
   int      stage1_items_per_cta;  /* vb_stage1_opts.items_per_cta */
+  int64_t  slab_pix;       /* > 0 and < npix: stream the sky through the device in slabs of this
+                              many pixels (a multiple of 1024 and of viss_tile_pix); run with
+                              vb_pipeline_run_host.  0: the whole sky is resident */
   int      use_graph;      /* 1: capture stages in one CUDA graph */
   int      device;         /* CUDA device ordinal */
 } vb_run_config;

@@ -151,3 +151,28 @@ def test_multi_day_running_sum_and_resume(gpu, vb, tmp_path):
     assert not (c / "C3day1M.bin").exists()
     acc2 = np.fromfile(c / "sum.bin", dtype=np.float32)
     assert np.abs(acc2 - acc).max() <= 1e-6 * np.abs(ref).max()
+
+
+def test_dropin_sky_slab_streaming(gpu, vb, tmp_path):
+    """--slab_pix streams the sky through the device (vb_pipeline_run_host in
+    slabs): same C as the resident run to summation rounding, and the running
+    sum works across slabs."""
+    exe = BIN / "main_recon_online_mirror_tile_vissfast"
+    sky = tmp_path / "sky"
+    common = ["--btag=1M", "--nside=16", "--segs=2", "--blockage=1", "--occ_mode=2", f"--sky_dir={sky}", "--gpus=0",
+              "--B_mode=bin", "--C_mode=bin", "--orbit_seed=42", "--sky_gen=4", "--day_start=1", "--day_count=2"]
+    a, b = tmp_path / "a", tmp_path / "b"
+    r = run(exe, common + [f"--out_dir={a}/"], tmp_path)
+    assert r.returncode == 0, r.stderr
+    r = run(exe, common + [f"--out_dir={b}/", "--slab_pix=1024", f"--accum_file={b}/sum.bin", "--autotune=1"],
+            tmp_path)
+    assert r.returncode == 0, r.stderr
+    assert "Autotune skipped" in r.stdout
+    for d in (1, 2):
+        Ca = np.fromfile(a / f"C{d}day1M.bin", dtype=np.float32)
+        Cb = np.fromfile(b / f"C{d}day1M.bin", dtype=np.float32)
+        e = rel_err(Cb, Ca)
+        assert e[0] < 1e-6 and e[1] < 1e-6, (d, e)
+    acc = np.fromfile(b / "sum.bin", dtype=np.float32)
+    ref = sum(np.fromfile(b / f"C{d}day1M.bin", dtype=np.float32).astype(np.float64) for d in (1, 2))
+    assert np.abs(acc - ref).max() <= 1e-6 * np.abs(ref).max()

@@ -75,7 +75,7 @@ class RunConfig(C.Structure):
                 ("seg_min_half", C.c_int), ("seg_max_half", C.c_int), ("seg_seed", C.c_uint64),
                 ("stage2_cull", C.c_int), ("stage2_ppt", C.c_int), ("stage2_items_per_cta", C.c_int),
                 ("stage1_bpt", C.c_int), ("stage1_stage_pix", C.c_int), ("stage1_ctas_per_sm", C.c_int),
-                ("stage1_items_per_cta", C.c_int), ("use_graph", C.c_int), ("device", C.c_int)]
+                ("stage1_items_per_cta", C.c_int), ("slab_pix", C.c_int64), ("use_graph", C.c_int), ("device", C.c_int)]
 
 
 class Report(C.Structure):

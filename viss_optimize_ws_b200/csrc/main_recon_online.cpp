@@ -193,6 +193,8 @@ int main(int argc, char** argv) {
   // viss_monitor.py / combine.py), kept on the device in FP64
   std::string accum_file = get_arg(argc, argv, "--accum_file", "");
   int keep_daily = to_int(get_arg(argc, argv, "--keep_daily", "1"), 1);
+  // stream the sky through the device in slabs of this many pixels (0: resident)
+  long long slab_pix = (long long)to_u64(get_arg(argc, argv, "--slab_pix", "0"), 0);
 
   if (btag != "1M" && btag != "10M" && btag != "30M") return die("ERROR --btag");
   if (nside <= 0) nside = (btag == "1M") ? 512 : (btag == "10M" ? 4096 : 16384);
@@ -284,6 +286,7 @@ int main(int argc, char** argv) {
   cfg.seg_max_half = seg_max;
   cfg.seg_seed = seg_seed;
   cfg.stage2_cull = stage2_cull;
+  cfg.slab_pix = slab_pix;
   cfg.use_graph = use_graph;
   cfg.device = 0;
 
@@ -300,7 +303,8 @@ int main(int argc, char** argv) {
     t_init.tic();
     if (!p) {
       if (vb_pipeline_create(&cfg, &p) != VB_OK) return die(std::string("ERROR ") + vb_last_error());
-      if (vb_pipeline_set_sky(p, hB.data(), 1) != VB_OK) return die(std::string("ERROR ") + vb_last_error());
+      if (!slab_pix && vb_pipeline_set_sky(p, hB.data(), 1) != VB_OK)
+        return die(std::string("ERROR ") + vb_last_error());
       if (!accum_file.empty()) {
         // resume from an existing running sum (float32, npix) or start at zero
         if (vb_malloc(reinterpret_cast<void**>(&d_acc), (size_t)npix * sizeof(double)) != VB_OK)
@@ -356,7 +360,8 @@ int main(int argc, char** argv) {
     int rc = vb_pipeline_make_baselines(p);
     if (rc == VB_ERR_HALFSYM) return die(std::string("ERROR: generated segment uvw does not satisfy half-sym: ") + vb_last_error());
     if (rc != VB_OK) return die(std::string("ERROR ") + vb_last_error());
-    if (autotune && di == 0) {
+    if (autotune && di == 0 && slab_pix) std::cout << "Autotune skipped: not available in sky-slab mode\n";
+    if (autotune && di == 0 && !slab_pix) {
       // kernel shapes for this workload, kept for the following days
       vb_tune_report tr{};
       if (vb_pipeline_autotune(p, 2, &tr) != VB_OK) return die(std::string("ERROR autotune: ") + vb_last_error());
@@ -379,7 +384,15 @@ int main(int argc, char** argv) {
     Timer t_rec;
     t_rec.tic();
     vb_report rep;
-    if (vb_pipeline_run(p, &rep) != VB_OK) return die(std::string("ERROR ") + vb_last_error());
+    std::vector<float> Cslab;
+    if (slab_pix) {
+      // sky-slab mode: B streams from host memory, C comes back slab by slab
+      Cslab.resize((size_t)npix);
+      if (vb_pipeline_run_host(p, hB.data(), 1, Cslab.data(), nullptr, &rep) != VB_OK)
+        return die(std::string("ERROR ") + vb_last_error());
+    } else if (vb_pipeline_run(p, &rep) != VB_OK) {
+      return die(std::string("ERROR ") + vb_last_error());
+    }
     std::vector<vb_seg_params> sp(nseg);
     vb_pipeline_seg_params(p, sp.data());
     Dev dv{p};
@@ -442,7 +455,7 @@ int main(int argc, char** argv) {
 
     Timer t_w;
     t_w.tic();
-    std::vector<float> Cout = dv.get("C");
+    std::vector<float> Cout = slab_pix ? std::move(Cslab) : dv.get("C");
     const bool txt = (C_mode == "txt");
     std::string outC = out_dir + "C" + dtag + (txt ? ".txt" : ".bin");
     if (d_acc) {
@@ -451,9 +464,19 @@ int main(int argc, char** argv) {
       t_a.tic();
       void* dC = nullptr;
       int64_t nC = 0;
-      if (vb_pipeline_device_ptr(p, "C", &dC, &nC) != VB_OK ||
-          vb_accumulate(static_cast<const float*>(dC), nC, d_acc, nullptr) != VB_OK || vb_synchronize() != VB_OK)
+      if (vb_pipeline_device_ptr(p, "C", &dC, &nC) != VB_OK) return die(std::string("ERROR ") + vb_last_error());
+      if (slab_pix) {
+        // the device holds one slab of C: add the host copy slab-sized piece by piece
+        for (int64_t b0 = 0; b0 < npix; b0 += nC) {
+          const int64_t cnt = std::min<int64_t>(nC, npix - b0);
+          if (vb_memcpy(dC, Cout.data() + b0, (size_t)cnt * sizeof(float), VB_H2D) != VB_OK ||
+              vb_accumulate(static_cast<const float*>(dC), cnt, d_acc + b0, nullptr) != VB_OK)
+            return die(std::string("ERROR ") + vb_last_error());
+        }
+      } else if (vb_accumulate(static_cast<const float*>(dC), nC, d_acc, nullptr) != VB_OK) {
         return die(std::string("ERROR ") + vb_last_error());
+      }
+      if (vb_synchronize() != VB_OK) return die(std::string("ERROR ") + vb_last_error());
       std::vector<double> a((size_t)npix);
       if (vb_memcpy(a.data(), d_acc, a.size() * sizeof(double), VB_D2H) != VB_OK)
         return die(std::string("ERROR ") + vb_last_error());

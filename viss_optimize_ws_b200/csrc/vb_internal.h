@@ -66,9 +66,10 @@ struct Stage1Buffers {       // slices of a workspace
 int stage1_plan(const vb_sky* sky, const vb_baselines* bl, const vb_stage1_opts* o, Stage1Plan* p);
 size_t stage1_carve(const Stage1Plan& p, void* ws, size_t cap, Stage1Buffers* b, bool pack_pixels);
 // pixels_ready: lm/nb/f4 (and cones for VB_CULL_EXACT) already hold this sky.
+// accumulate: V_half += this sky's sum (slabs of one sky) instead of V_half =.
 int stage1_run(const vb_sky* sky, const vb_baselines* bl, const Stage1Plan& p, const Stage1Buffers& b,
                bool pixels_ready, double* V_half, unsigned long long* counters, cudaStream_t s,
-               cudaEvent_t kbeg = nullptr, cudaEvent_t kend = nullptr);
+               cudaEvent_t kbeg = nullptr, cudaEvent_t kend = nullptr, bool accumulate = false);
 int stage1_prepare_pixels(const vb_sky* sky, const Stage1Plan& p, const Stage1Buffers& b, cudaStream_t s);
 int phase_correct_expand_async(const double* Vraw, const float* w_full, int n_half, int nbl,
                                int already_corrected, float* Vh, float* Vf, cudaStream_t s);

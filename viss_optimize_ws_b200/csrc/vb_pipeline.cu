@@ -83,6 +83,11 @@ struct vb_pipeline {
   vb_run_config cfg{};
   cudaStream_t s = nullptr;
   int64_t npix = 0;
+  // sky-slab streaming: nres = pixels resident on the device (npix, or the
+  // slab size when the sky is streamed in nslab slabs from host memory)
+  int nside = 0;
+  int64_t nres = 0;
+  int nslab = 1;
   float cosphi = 0.f;
   bool per_end_cosphi = false;
   // sky
@@ -103,6 +108,7 @@ struct vb_pipeline {
   bool baselines_ready = false;
   float auto_bl_max = 0.f;       // bl_max_m <= 0: measured by make_baselines
   unsigned* d_uvmax = nullptr;   // scratch of that measurement
+  unsigned* slab_err = nullptr;  // stage-1 error word in sky-slab mode
   // stage 1
   Stage1Plan p1{};
   void* ws1 = nullptr;
@@ -216,7 +222,7 @@ static void drop_graph(vb_pipeline* p) {
 
 static vb_sky sky_of(const vb_pipeline* p) {
   vb_sky k{};
-  k.npix = p->npix;
+  k.npix = p->nres;
   k.B = p->B; k.l = p->l; k.m = p->m; k.n = p->n;
   k.tile_pix = p->tile_pix;
   k.cx = p->cx; k.cy = p->cy; k.cz = p->cz; k.cosA = p->cosA; k.sinA = p->sinA;
@@ -285,6 +291,17 @@ static int uneven_total_steps(const vb_run_config& c, int nbl) {
 
 static int plan_stages(vb_pipeline* p);
 
+// Pixel geometry of pixels [base, base + count) into the resident arrays:
+// l, m, n (NEST), n - 1 and the tile-cone meta of the slab's tiles.
+static int slab_geometry(vb_pipeline* p, int64_t base, int64_t count) {
+  if (base > UINT32_MAX) return fail(VB_ERR_UNSUPPORTED, "slab base %lld beyond 32-bit pixel indices", (long long)base);
+  VB_TRY(vb_pix2lmn_nest(p->nside, (uint32_t)base, count, p->l, p->m, p->n, p->s));
+  VB_TRY(vb_build_nm1(p->n, p->nm1, count, p->s));
+  if (p->tile_pix)
+    VB_TRY(vb_tile_cone_meta(p->tile_pix, p->l, p->m, p->n, count, p->cx, p->cy, p->cz, p->cosA, p->sinA, p->s));
+  return VB_OK;
+}
+
 static vb_orbit_params orbit_params_of(const vb_run_config& c) {
   vb_orbit_params op{};
   op.model = c.orbit_model;
@@ -344,28 +361,38 @@ extern "C" int vb_pipeline_create(const vb_run_config* c, vb_pipeline** out) {
   }
   p->per_end_cosphi = c->occ_R_m > 0.0;
 
-  // sky geometry
+  // sky geometry (all of it, or one slab at a time)
   const int nside = c->nside;
+  p->nside = nside;
   p->npix = 12LL * nside * nside;
-  PTRY(dalloc(p, &p->B, p->npix));
-  PTRY(dalloc(p, &p->l, p->npix));
-  PTRY(dalloc(p, &p->m, p->npix));
-  PTRY(dalloc(p, &p->n, p->npix));
-  PTRY(dalloc(p, &p->nm1, p->npix));
-  PCUDA(cudaMemsetAsync(p->B, 0, p->npix * sizeof(float), p->s));
-  PTRY(vb_pix2lmn_nest(nside, 0, p->npix, p->l, p->m, p->n, p->s));
-  PTRY(vb_build_nm1(p->n, p->nm1, p->npix, p->s));
+  p->nres = p->npix;
   if (c->cull == VB_CULL_TILECONE && c->blockage) {
     p->tile_pix = c->viss_tile_pix > 0 ? c->viss_tile_pix : 256;
     if (p->tile_pix & (p->tile_pix - 1)) PTRY(fail(VB_ERR_INVALID, "viss_tile_pix=%d must be a power of two", p->tile_pix));
-    p->ntile = (int)ceil_div(p->npix, p->tile_pix);
+  }
+  if (c->slab_pix > 0 && c->slab_pix < p->npix) {
+    // slabs hold whole cull tiles and stage-2 pixel blocks (multiples of 1024)
+    const int64_t unit = std::max<int64_t>(1024, p->tile_pix);
+    if (c->slab_pix % unit != 0)
+      PTRY(fail(VB_ERR_INVALID, "slab_pix=%lld must be a multiple of %lld", (long long)c->slab_pix, (long long)unit));
+    p->nres = c->slab_pix;
+    p->nslab = (int)ceil_div(p->npix, p->nres);
+  }
+  PTRY(dalloc(p, &p->B, p->nres));
+  PTRY(dalloc(p, &p->l, p->nres));
+  PTRY(dalloc(p, &p->m, p->nres));
+  PTRY(dalloc(p, &p->n, p->nres));
+  PTRY(dalloc(p, &p->nm1, p->nres));
+  PCUDA(cudaMemsetAsync(p->B, 0, p->nres * sizeof(float), p->s));
+  if (p->tile_pix) {
+    p->ntile = (int)ceil_div(p->nres, p->tile_pix);
     PTRY(dalloc(p, &p->cx, p->ntile));
     PTRY(dalloc(p, &p->cy, p->ntile));
     PTRY(dalloc(p, &p->cz, p->ntile));
     PTRY(dalloc(p, &p->cosA, p->ntile));
     PTRY(dalloc(p, &p->sinA, p->ntile));
-    PTRY(vb_tile_cone_meta(p->tile_pix, p->l, p->m, p->n, p->npix, p->cx, p->cy, p->cz, p->cosA, p->sinA, p->s));
   }
+  if (p->nslab == 1) PTRY(slab_geometry(p, 0, p->npix));
 
   // orbit generator
   vb_orbit_params op = orbit_params_of(*c);
@@ -395,8 +422,8 @@ extern "C" int vb_pipeline_create(const vb_run_config* c, vb_pipeline** out) {
   PTRY(dalloc(p, &p->Vd, (size_t)2 * p->n_half));
   PTRY(dalloc(p, &p->Vh, (size_t)2 * p->n_half));
   PTRY(dalloc(p, &p->Vf, (size_t)2 * p->n_full));
-  PTRY(dalloc(p, &p->C, p->npix));
-  PTRY(dalloc(p, &p->W, p->npix));
+  PTRY(dalloc(p, &p->C, p->nres));
+  PTRY(dalloc(p, &p->W, p->nres));
   PTRY(dalloc(p, &p->segp, p->nseg));
   PTRY(dalloc(p, &p->wsum, 2));
   PTRY(dalloc(p, &p->counters, 8));
@@ -415,6 +442,9 @@ __global__ void k_scale_sky(float* B, int64_t n, double scale) {
 
 static int set_sky_async(vb_pipeline* p, const float* B_host, int scale) {
   if (!B_host) return fail(VB_ERR_INVALID, "set_sky: null B");
+  if (p->nslab > 1)
+    return fail(VB_ERR_UNSUPPORTED, "sky-slab mode (%d slabs): the sky streams from host memory through "
+                "vb_pipeline_run_host", p->nslab);
   VB_CUDA(cudaMemcpyAsync(p->B, B_host, p->npix * sizeof(float), cudaMemcpyHostToDevice, p->s));
   if (scale) {
     // B *= 4 pi / npix in FP64 (main_recon_online.cu:106-112)
@@ -545,7 +575,7 @@ static int plan_stages(vb_pipeline* p) {
   o2.bl_max = effective_bl_max(p);
   o2.lambda = c->lambda_m;
   Stage2Plan p2;
-  VB_TRY(stage2_plan(p->n_half, p->nseg, p->npix, &o2, &p2));
+  VB_TRY(stage2_plan(p->n_half, p->nseg, p->nres, &o2, &p2));
   drop_graph(p);
   if (p->s) VB_CUDA(cudaStreamSynchronize(p->s));
   VB_TRY(regrow(p, &p->ws1, &p->ws1_bytes, stage1_carve(p1, nullptr, 0, nullptr, true)));
@@ -653,6 +683,7 @@ static int run_once(vb_pipeline* p) {
 
 extern "C" int vb_pipeline_run(vb_pipeline* p, vb_report* r) {
   if (!p) return fail(VB_ERR_INVALID, "vb_pipeline_run: null pipeline");
+  if (p->nslab > 1) return fail(VB_ERR_UNSUPPORTED, "sky-slab mode: use vb_pipeline_run_host");
   VB_CUDA(cudaSetDevice(p->cfg.device));
   VB_TRY(ensure_ready(p));
   VB_TRY(run_once(p));
@@ -661,10 +692,105 @@ extern "C" int vb_pipeline_run(vb_pipeline* p, vb_report* r) {
   return VB_OK;
 }
 
+// Sky-slab streaming (nslab > 1): stage 1 sums slab by slab into one V
+// (pixel geometry generated per slab, B copied from host memory per slab);
+// stage 2 then rebuilds the (small) group tables per slab and writes each
+// slab's C straight back to host memory.  Device memory holds one slab.
+static int run_slabs(vb_pipeline* p, const float* B_host, int scale, float* C_host, float* V_half_host,
+                     vb_report* r) {
+  if (!B_host) return fail(VB_ERR_INVALID, "vb_pipeline_run_host: null B");
+  VB_CUDA(record_event(p->ev[3], p->s));
+  VB_TRY(make_baselines_async(p));
+  if (p->cfg.bl_max_m <= 0.f && !(p->auto_bl_max > 0.f)) VB_TRY(measure_bl_max(p));
+  p->baselines_ready = true;
+  vb_baselines bl = bl_of(p);
+  VB_CUDA(cudaMemsetAsync(p->counters, 0, 8 * sizeof(unsigned long long), p->s));
+  // one stage-1 error word for all slabs (the slab plans carve the workspace differently)
+  if (!p->slab_err) VB_TRY(dalloc(p, &p->slab_err, 1));
+  p->b1.err = p->slab_err;
+  VB_CUDA(cudaMemsetAsync(p->slab_err, 0, sizeof(unsigned), p->s));
+  const double pix_area = 4.0 * 3.14159265358979323846 / (double)p->npix;
+  vb_stage1_opts o1{};
+  o1.precision = p->cfg.precision;
+  o1.cull = p->cfg.cull;
+  o1.phase_corrected = 1;
+  o1.blockage = p->cfg.blockage;
+  o1.bpt = p->cfg.stage1_bpt;
+  o1.stage_pix = p->cfg.stage1_stage_pix;
+  o1.ctas_per_sm = p->cfg.stage1_ctas_per_sm;
+  o1.items_per_cta = p->cfg.stage1_items_per_cta;
+  VB_CUDA(record_event(p->ev[0], p->s));
+  for (int k = 0; k < p->nslab; ++k) {
+    const int64_t base = (int64_t)k * p->nres;
+    const int64_t cnt = std::min<int64_t>(p->nres, p->npix - base);
+    VB_TRY(slab_geometry(p, base, cnt));
+    VB_CUDA(cudaMemcpyAsync(p->B, B_host + base, cnt * sizeof(float), cudaMemcpyHostToDevice, p->s));
+    if (scale) {
+      int g = (int)std::min<int64_t>(ceil_div(cnt, 256), (int64_t)sm_count() * 16);
+      k_scale_sky<<<g, 256, 0, p->s>>>(p->B, cnt, pix_area);
+      VB_LAUNCH_CHECK();
+    }
+    vb_sky sky = sky_of(p);
+    sky.npix = cnt;
+    Stage1Plan q;
+    VB_TRY(stage1_plan(&sky, &bl, &o1, &q));
+    Stage1Buffers b;
+    if (!stage1_carve(q, p->ws1, p->ws1_bytes, &b, true))
+      return fail(VB_ERR_NOMEM, "slab %d: stage-1 workspace too small", k);
+    b.err = p->slab_err;
+    VB_TRY(stage1_run(&sky, &bl, q, b, false, p->Vd, p->counters, p->s, nullptr, nullptr, k > 0));
+  }
+  VB_TRY(phase_correct_expand_async(p->Vd, p->w, p->n_half, p->nbl, 1, p->Vh, p->Vf, p->s));
+  VB_CUDA(record_event(p->ev[1], p->s));
+  vb_stage2_opts o2{};
+  o2.mirror = p->cfg.mirror;
+  o2.blockage = p->cfg.blockage;
+  o2.occ_mode = p->cfg.occ_mode;
+  o2.precision = p->cfg.precision;
+  o2.cull = p->cfg.stage2_cull;
+  o2.ppt = p->cfg.stage2_ppt;
+  o2.items_per_cta = p->cfg.stage2_items_per_cta;
+  o2.grid_res = p->cfg.grid_res;
+  o2.bl_max = effective_bl_max(p);
+  o2.lambda = p->cfg.lambda_m;
+  for (int k = 0; k < p->nslab; ++k) {
+    const int64_t base = (int64_t)k * p->nres;
+    const int64_t cnt = std::min<int64_t>(p->nres, p->npix - base);
+    VB_TRY(slab_geometry(p, base, cnt));
+    vb_sky sky = sky_of(p);
+    sky.npix = cnt;
+    Stage2Plan q;
+    VB_TRY(stage2_plan(p->n_half, p->nseg, cnt, &o2, &q));
+    VB_TRY(stage2_run(&sky, &bl, p->Vh, p->nseg, p->d_t0, p->d_tlen, q, p->ws2, p->ws2_bytes, p->C, p->W, p->segp,
+                      p->counters + 4, p->wsum, p->s, nullptr));
+    VB_CUDA(cudaMemcpyAsync(C_host + base, p->C, cnt * sizeof(float), cudaMemcpyDeviceToHost, p->s));
+  }
+  VB_CUDA(record_event(p->ev[2], p->s));
+  if (V_half_host)
+    VB_CUDA(cudaMemcpyAsync(V_half_host, p->Vh, (size_t)2 * p->n_half * sizeof(float), cudaMemcpyDeviceToHost, p->s));
+  VB_CUDA(record_event(p->ev[4], p->s));
+  // the per-kernel events cover the whole stage here
+  VB_CUDA(record_event(p->ev[5], p->s));
+  VB_CUDA(record_event(p->ev[6], p->s));
+  VB_CUDA(record_event(p->ev[7], p->s));
+  VB_CUDA(record_event(p->ev[8], p->s));
+  VB_CUDA(cudaStreamSynchronize(p->s));
+  VB_TRY(fill_report(p, r));
+  if (r) {
+    float te = 0.f;
+    VB_CUDA(cudaEventElapsedTime(&te, p->ev[3], p->ev[4]));
+    r->t_e2e_ms = te;
+    r->t_s1_kernel_ms = r->t_stage1_ms;
+    r->t_s2_kernel_ms = r->t_stage2_ms;
+  }
+  return VB_OK;
+}
+
 extern "C" int vb_pipeline_run_host(vb_pipeline* p, const float* B_host, int scale, float* C_host,
                                     float* V_half_host, vb_report* r) {
   if (!p || !C_host) return fail(VB_ERR_INVALID, "vb_pipeline_run_host: null argument");
   VB_CUDA(cudaSetDevice(p->cfg.device));
+  if (p->nslab > 1) return run_slabs(p, B_host, scale, C_host, V_half_host, r);
   VB_CUDA(record_event(p->ev[3], p->s));
   VB_TRY(set_sky_async(p, B_host, scale));
   VB_TRY(make_baselines_async(p));
@@ -692,15 +818,15 @@ extern "C" int vb_pipeline_device_ptr(vb_pipeline* p, const char* name, void** p
   if (!p || !name || !ptr) return fail(VB_ERR_INVALID, "vb_pipeline_device_ptr: null argument");
   struct E { const char* k; void* v; int64_t n; };
   const E tab[] = {
-      {"C", p->C, p->npix}, {"W", p->W, p->npix}, {"V_half", p->Vh, 2LL * p->n_half},
+      {"C", p->C, p->nres}, {"W", p->W, p->nres}, {"V_half", p->Vh, 2LL * p->n_half},
       {"V_full", p->Vf, 2LL * p->n_full}, {"V_half_d", p->Vd, 2LL * p->n_half},
       {"u", p->u, p->n_full}, {"v", p->v, p->n_full}, {"w", p->w, p->n_full},
       {"x1", p->x1, p->n_full}, {"y1", p->y1, p->n_full}, {"z1", p->z1, p->n_full},
       {"x2", p->x2, p->n_full}, {"y2", p->y2, p->n_full}, {"z2", p->z2, p->n_full},
       {"invn1", p->in1, p->n_full}, {"invn2", p->in2, p->n_full},
       {"cosphi1", p->cp1, p->cp1 ? p->n_full : 0}, {"cosphi2", p->cp2, p->cp2 ? p->n_full : 0},
-      {"l", p->l, p->npix}, {"m", p->m, p->npix}, {"n", p->n, p->npix}, {"B", p->B, p->npix},
-      {"nm1", p->nm1, p->npix}, {"cx", p->cx, p->ntile}, {"cy", p->cy, p->ntile}, {"cz", p->cz, p->ntile},
+      {"l", p->l, p->nres}, {"m", p->m, p->nres}, {"n", p->n, p->nres}, {"B", p->B, p->nres},
+      {"nm1", p->nm1, p->nres}, {"cx", p->cx, p->ntile}, {"cy", p->cy, p->ntile}, {"cz", p->cz, p->ntile},
       {"cosA", p->cosA, p->ntile}, {"sinA", p->sinA, p->ntile}, {"seg_t0", p->d_t0, p->nseg},
       {"seg_tlen", p->d_tlen, p->nseg}, {"seg_params", p->segp, p->nseg},
   };
@@ -765,6 +891,7 @@ static int time_stages(vb_pipeline* p, int reps, double* k1, double* k2) {
 extern "C" int vb_pipeline_autotune(vb_pipeline* p, int reps, vb_tune_report* out) {
   if (!p) return fail(VB_ERR_INVALID, "vb_pipeline_autotune: null pipeline");
   if (!p->sky_set) return fail(VB_ERR_INVALID, "vb_pipeline_autotune: sky not set");
+  if (p->nslab > 1) return fail(VB_ERR_UNSUPPORTED, "vb_pipeline_autotune: not in sky-slab mode");
   VB_CUDA(cudaSetDevice(p->cfg.device));
   if (reps <= 0) reps = 2;
   vb_tune_report t{};

@@ -403,9 +403,9 @@ __global__ void __maxnreg__(MINB == 3 ? 80 : 120) k_stage1(const S1Args a) {
   if (a.counters && threadIdx.x < 4) atomicAdd(&a.counters[threadIdx.x], s_cnt[threadIdx.x]);
 }
 
-// V[ih] = sum over chunks of the partials, in chunk order.
+// V[ih] = sum over chunks of the partials, in chunk order (accumulate: V += that sum).
 __global__ void k_reduce_partials(const double2* __restrict__ partial, int nchunk, int n_half,
-                                  double* __restrict__ V) {
+                                  double* __restrict__ V, int accumulate) {
   for (int ih = blockIdx.x * blockDim.x + threadIdx.x; ih < n_half; ih += gridDim.x * blockDim.x) {
     double r = 0.0, im = 0.0;
     for (int c = 0; c < nchunk; ++c) {
@@ -413,8 +413,13 @@ __global__ void k_reduce_partials(const double2* __restrict__ partial, int nchun
       r += p.x;
       im += p.y;
     }
-    V[2 * ih] = r;
-    V[2 * ih + 1] = im;
+    if (accumulate) {
+      V[2 * ih] += r;
+      V[2 * ih + 1] += im;
+    } else {
+      V[2 * ih] = r;
+      V[2 * ih + 1] = im;
+    }
   }
 }
 
@@ -582,7 +587,7 @@ int stage1_prepare_pixels(const vb_sky* sky, const Stage1Plan& p, const Stage1Bu
 
 int stage1_run(const vb_sky* sky, const vb_baselines* bl, const Stage1Plan& p, const Stage1Buffers& b,
                bool pixels_ready, double* V_half, unsigned long long* counters, cudaStream_t s, cudaEvent_t kbeg,
-               cudaEvent_t kend) {
+               cudaEvent_t kend, bool accumulate) {
   if (p.n_half == 0) return VB_OK;
   if (!pixels_ready) VB_TRY(stage1_prepare_pixels(sky, p, b, s));
   S1Args a{};
@@ -608,7 +613,7 @@ int stage1_run(const vb_sky* sky, const vb_baselines* bl, const Stage1Plan& p, c
   if (kend) VB_CUDA(record_event(kend, s));
   int rg = (int)ceil_div(p.n_half, 256);
   if (rg > sm_count() * 16) rg = sm_count() * 16;
-  k_reduce_partials<<<rg, 256, 0, s>>>(b.partial, p.nchunk, p.n_half, V_half);
+  k_reduce_partials<<<rg, 256, 0, s>>>(b.partial, p.nchunk, p.n_half, V_half, accumulate ? 1 : 0);
   VB_LAUNCH_CHECK();
   return VB_OK;
 }
