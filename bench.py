@@ -477,6 +477,18 @@ def run_config_report(args) -> None:
             "stage2_sfu_frac": (r["s2_counters"][0] + r["s2_counters"][1]) / (t["t_s2_kernel_ms"] * 1e-3) / 1e9 / peak,
             "err_V": ev, "err_C": ec, "W_equal_fp64": bool(np.array_equal(p.get("W"), W64)),
             "error_flags": r["error_flags"], "autotune": tune}
+        if prec == "fp32_fp64phase" and n == 5:
+            # end to end from host memory, resident sky against sky-slab streaming (4 slabs)
+            Cr, _, rr = p.run_host(B)
+            Cr, _, rr = p.run_host(B)
+            slab = kw["nside"] ** 2 * 3
+            with vb.Pipeline(vb.run_config(slab_pix=slab, **config_kwargs(n, prec))) as ps:
+                ps.run_host(B)
+                Cs, _, rs = ps.run_host(B)
+            out["sky_slab_streaming"] = {"slab_pix": slab, "slabs": 4, "e2e_resident_ms": rr["t_e2e_ms"],
+                                         "e2e_slab_ms": rs["t_e2e_ms"], "C_vs_resident": err_report(Cs, Cr, False),
+                                         "counters_equal": rr["s1_counters"] == rs["s1_counters"]
+                                         and rr["s2_counters"] == rs["s2_counters"]}
         if prec == "fp32_fp64phase" and n == 4:
             loop = per_segment_loop(vb, p, shapes, 2)
             out["per_segment_loop"] = {"ms_per_step": loop["ms_per_step"], "launch_calls": loop["launch_calls"],
