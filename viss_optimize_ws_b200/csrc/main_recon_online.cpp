@@ -22,12 +22,15 @@
 #include <fstream>
 #include <iomanip>
 #include <iostream>
+#include <memory>
+#include <mutex>
 #include <random>
 #include <sstream>
 #include <string>
 #include <vector>
 
 #include "vissb200.h"
+#include "vb_text.h"
 
 #if !defined(VB_DEFAULTS_ROOT) && !defined(VB_DEFAULTS_VISSFAST)
 #define VB_DEFAULTS_ROOT 1
@@ -110,11 +113,8 @@ bool load_B_auto(const std::string& dir, const std::string& btag, float* out, lo
   return tb(b1) || tb(b2) || tt(t1) || tt(t2);
 }
 
-void write_3cols(std::ofstream& ofs, const float* a, const float* b, const float* c, size_t n) {
-  ofs.setf(std::ios::scientific);
-  ofs << std::setprecision(15);
-  for (size_t i = 0; i < n; ++i) ofs << (double)a[i] << " " << (double)b[i] << " " << (double)c[i] << "\n";
-}
+// Failed writes are reported on stderr when the writer is drained.
+std::string write_error(const std::string& path) { return "ERROR writing " + path + "\n"; }
 
 struct Dev {
   vb_pipeline* p;
@@ -193,6 +193,8 @@ int main(int argc, char** argv) {
   // viss_monitor.py / combine.py), kept on the device in FP64
   std::string accum_file = get_arg(argc, argv, "--accum_file", "");
   int keep_daily = to_int(get_arg(argc, argv, "--keep_daily", "1"), 1);
+  // write each day's files on a background thread while the next day computes
+  int async_write = to_int(get_arg(argc, argv, "--async_write", "1"), 1);
   // stream the sky through the device in slabs of this many pixels (0: resident)
   long long slab_pix = (long long)to_u64(get_arg(argc, argv, "--slab_pix", "0"), 0);
 
@@ -293,11 +295,13 @@ int main(int argc, char** argv) {
   std::ostringstream json;
   json << "{\"days\": [";
   // one run context for all days: each further day only swaps the orbit
+  vbtext::AsyncWriter writer(async_write != 0);
   vb_pipeline* p = nullptr;
   double* d_acc = nullptr;
   for (int di = 0; di < day_count; ++di) {
     const int dayid = day_start + di;
     cfg.day = dayid;
+    writer.drain(std::cout);
     if (vissfast) std::cout << "===== Day " << dayid << " / " << (day_start + day_count - 1) << " =====\n";
     Timer t_init;
     t_init.tic();
@@ -400,25 +404,36 @@ int main(int argc, char** argv) {
     if (print_stats || write_baseline_txt) { hu = dv.get("u"); hv = dv.get("v"); hw = dv.get("w"); }
     const std::string dtag = std::to_string(dayid) + "day" + btag;
     if (write_viss) {
+      // "re im" per signed baseline, printf %g as the upstream iostream output
       std::string fv = out_dir + "Viss" + dtag + ".txt";
-      std::ofstream ofs(fv);
-      if (!ofs.is_open()) return die("ERROR open " + fv);
       std::cout << "Will stream phase-corrected Viss to " << fv << "\n";
-      std::vector<float> Vf = dv.get("V_full");
-      std::vector<char> buf(8 << 20);
-      ofs.rdbuf()->pubsetbuf(buf.data(), buf.size());
-      for (size_t i = 0; i + 1 < Vf.size(); i += 2) ofs << Vf[i] << " " << Vf[i + 1] << "\n";
+      auto Vf = std::make_shared<std::vector<float>>(dv.get("V_full"));
+      writer.submit([&writer, fv, Vf] {
+        const bool ok = vbtext::write_rows(fv, {{Vf->data(), 2}, {Vf->data() + 1, 2}}, Vf->size() / 2,
+                                           vbtext::Fmt::General6);
+        if (!ok) writer.log(write_error(fv));
+        return ok;
+      });
     }
     if (write_baseline_txt) {
-      std::ofstream a(out_dir + "uvw" + dtag + ".txt"), b(out_dir + "xyza" + dtag + ".txt"),
-          c(out_dir + "xyzb" + dtag + ".txt");
-      if (!a.is_open() || !b.is_open() || !c.is_open()) return die("ERROR open generated baseline txt outputs");
       std::cout << "Will stream generated uvw/xyza/xyzb to txt under " << out_dir << "\n";
-      std::vector<float> x1 = dv.get("x1"), y1 = dv.get("y1"), z1 = dv.get("z1");
-      std::vector<float> x2 = dv.get("x2"), y2 = dv.get("y2"), z2 = dv.get("z2");
-      write_3cols(a, hu.data(), hv.data(), hw.data(), hu.size());
-      write_3cols(b, x1.data(), y1.data(), z1.data(), x1.size());
-      write_3cols(c, x2.data(), y2.data(), z2.data(), x2.size());
+      auto tab = std::make_shared<std::vector<std::vector<float>>>();
+      tab->push_back(hu);
+      tab->push_back(hv);
+      tab->push_back(hw);
+      for (const char* k : {"x1", "y1", "z1", "x2", "y2", "z2"}) tab->push_back(dv.get(k));
+      const std::string names[3] = {out_dir + "uvw" + dtag + ".txt", out_dir + "xyza" + dtag + ".txt",
+                                    out_dir + "xyzb" + dtag + ".txt"};
+      for (int f = 0; f < 3; ++f) {
+        const std::string fn = names[f];
+        writer.submit([&writer, fn, tab, f] {
+          const auto& t = *tab;
+          const bool ok = vbtext::write_rows(fn, {{t[3 * f].data(), 1}, {t[3 * f + 1].data(), 1}, {t[3 * f + 2].data(), 1}},
+                                             t[3 * f].size(), vbtext::Fmt::Sci15);
+          if (!ok) writer.log(write_error(fn));
+          return ok;
+        });
+      }
     }
     // per-segment lines: each segment's share of the batched stage times
     const double tot_s1 = (double)rep.n_half_total;
@@ -453,8 +468,6 @@ int main(int argc, char** argv) {
     }
     std::cout << "Recon done in " << t_rec.toc_s() << " s\n";
 
-    Timer t_w;
-    t_w.tic();
     std::vector<float> Cout = slab_pix ? std::move(Cslab) : dv.get("C");
     const bool txt = (C_mode == "txt");
     std::string outC = out_dir + "C" + dtag + (txt ? ".txt" : ".bin");
@@ -504,18 +517,23 @@ int main(int argc, char** argv) {
     }
     if (!keep_daily) {
       std::cout << "Daily C not written (--keep_daily=0)\n";
-    } else if (txt) {
-      std::ofstream ofs(outC);
-      if (!ofs.is_open()) return die("ERROR open " + outC);
-      std::vector<char> buf(8 << 20);
-      ofs.rdbuf()->pubsetbuf(buf.data(), buf.size());
-      for (float x : Cout) ofs << x << "\n";
     } else {
-      std::ofstream ofs(outC, std::ios::binary);
-      if (!ofs.is_open()) return die("ERROR open " + outC);
-      ofs.write(reinterpret_cast<const char*>(Cout.data()), (std::streamsize)(Cout.size() * sizeof(float)));
+      auto Ch = std::make_shared<std::vector<float>>(std::move(Cout));
+      writer.submit([&writer, outC, Ch, txt] {
+        Timer tw;
+        tw.tic();
+        const bool ok = txt ? vbtext::write_rows(outC, {{Ch->data(), 1}}, Ch->size(), vbtext::Fmt::General6)
+                            : vbtext::write_binary(outC, Ch->data(), Ch->size() * sizeof(float));
+        if (!ok) {
+          writer.log(write_error(outC));
+          return false;
+        }
+        std::ostringstream m;
+        m << "Wrote " << outC << " in " << tw.toc_s() << " s\n";
+        writer.log(m.str());
+        return true;
+      });
     }
-    if (keep_daily) std::cout << "Wrote " << outC << " in " << t_w.toc_s() << " s\n";
     json << (di ? ", " : "") << "{\"day\": " << dayid << ", \"t_stage1_ms\": " << rep.t_stage1_ms
          << ", \"t_stage2_ms\": " << rep.t_stage2_ms << ", \"stage1_terms\": " << rep.stage1_terms
          << ", \"stage2_terms\": " << rep.stage2_terms << ", \"groups\": " << rep.groups_total
@@ -523,6 +541,9 @@ int main(int argc, char** argv) {
   }
   if (p) vb_pipeline_destroy(p);
   if (d_acc) vb_free(d_acc);
+  const bool wrote = writer.wait();
+  writer.drain(std::cout);
+  if (!wrote) return die("ERROR writing outputs");
   json << "]}";
   if (!report_json.empty()) {
     std::ofstream o(report_json);
