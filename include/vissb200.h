@@ -188,6 +188,9 @@ typedef struct {
   int exact_tile_pix;   /* tile of the VB_CULL_EXACT cones (0 = auto) */
   int ctas_per_sm;      /* resident CTAs per SM the kernel is built for: 2, or 3 with bpt <= 2 (0 = 2) */
   int items_per_cta;    /* work-queue items per resident CTA when chunk_pix = 0 (0 = auto) */
+  int refine_pix;       /* tile-cone culling: inside mixed tiles, exact sub-tiles of this many
+                           pixels skip or drop the per-pixel test where they can (0 = 128,
+                           < 0 = off); results are identical either way */
 } vb_stage1_opts;
 
 size_t vb_stage1_workspace_bytes(const vb_sky* sky, const vb_baselines* bl,
@@ -340,6 +343,7 @@ typedef struct {
   int      stage1_stage_pix;      /* vb_stage1_opts.stage_pix */
   int      stage1_ctas_per_sm;    /* vb_stage1_opts.ctas_per_sm */
   int      stage1_items_per_cta;  /* vb_stage1_opts.items_per_cta */
+  int      stage1_refine_pix;     /* vb_stage1_opts.refine_pix */
   int64_t  slab_pix;       /* > 0 and < npix: stream the sky through the device in slabs of this
                               many pixels (a multiple of 1024 and of viss_tile_pix); run with
                               vb_pipeline_run_host.  0: the whole sky is resident */

@@ -121,10 +121,10 @@ def tile_meta(tile_pix: int, dl, dm, dn, npix: int):
 
 
 def stage1(sky, bls, *, precision, cull, phase_corrected=1, blockage=1, bpt=0, stage_pix=0, chunk_pix=0,
-           exact_tile_pix=0, ctas_per_sm=0, items_per_cta=0):
+           exact_tile_pix=0, ctas_per_sm=0, items_per_cta=0, refine_pix=0):
     o = vb.Stage1Opts(precision=precision, cull=cull, phase_corrected=phase_corrected, blockage=blockage, bpt=bpt,
                       stage_pix=stage_pix, chunk_pix=chunk_pix, exact_tile_pix=exact_tile_pix,
-                      ctas_per_sm=ctas_per_sm, items_per_cta=items_per_cta)
+                      ctas_per_sm=ctas_per_sm, items_per_cta=items_per_cta, refine_pix=refine_pix)
     need = vb.lib().vb_stage1_workspace_bytes(C.byref(sky), C.byref(bls), C.byref(o))
     assert need > 0, vb.lib().vb_last_error()
     ws = DeviceBuffer(need)

@@ -351,3 +351,17 @@ def test_library_kernel_masks_match_upstream(case, vb, ref, cull):
     mine = decode_my_masks(case, vb, cm)
     up = decode_upstream_masks(case, ref, "plain" if cull == "none" else "tilecone")
     assert np.array_equal(mine, up), f"{int((mine != up).sum())} differing (baseline, pixel) decisions"
+
+
+@pytest.mark.parametrize("prec", ["fp32_fp64phase", "fp64", "fp32_dsphase"])
+def test_tilecone_subtile_refinement_is_bit_identical(case, vb, prec):
+    """Exact sub-tiles inside tile-cone mixed tiles change only which path a
+    warp takes (skip / class select / per-pixel test): V is bit-identical with
+    refinement off, and the counters move terms from masked to fast / hidden."""
+    sky, bl = structs(case)
+    pm = {"fp64": vb.PREC_FP64, "fp32_fp64phase": vb.PREC_FP32_FP64PH, "fp32_dsphase": vb.PREC_FP32_DSPH}[prec]
+    Voff, coff = stage1(sky, bl, precision=pm, cull=vb.CULL_TILECONE, refine_pix=-1)
+    for r in (0, 32, 64, 128):
+        V, c = stage1(sky, bl, precision=pm, cull=vb.CULL_TILECONE, refine_pix=r)
+        assert np.array_equal(V.view(np.uint64), Voff.view(np.uint64)), r
+        assert c[3] == coff[3] and c[1] <= coff[1] and c[0] >= coff[0] and c[2] >= coff[2]

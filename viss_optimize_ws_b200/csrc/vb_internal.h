@@ -45,7 +45,7 @@ int geom_invnorm(const float* x, const float* y, const float* z, float* invn, in
 // ----- stage 1 ---------------------------------------------------------------
 struct Stage1Plan {
   int precision, cull, phase_corrected, blockage;
-  int bpt, minb, stage_pix, chunk_pix, cull_tile;
+  int bpt, minb, stage_pix, chunk_pix, cull_tile, refine_pix;
   int64_t npix;
   int n_half, nbl;
   int nchunk, n_btile, n_items, grid;
@@ -58,6 +58,7 @@ struct Stage1Buffers {       // slices of a workspace
   float4* nb = nullptr;
   float4* f4 = nullptr;
   ExactCone* cones = nullptr;
+  ExactCone* subcones = nullptr;   // tile-cone refinement sub-tiles
   double2* partial = nullptr;
   int* queue = nullptr;
   unsigned* err = nullptr;
