@@ -101,6 +101,9 @@ def parse() -> argparse.Namespace:
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 GPU comparison run")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--mode", default="replicas", choices=["replicas", "sharded"],
+                    help="N > 1: independent replicas (weak scaling, default) or one day split over the ranks "
+                         "(strong scaling: stage 1 by time steps + all-gather of V, stage 2 by pixels + gather of C)")
     ap.add_argument("--config", type=int, default=0,
                     help="print a report line for configuration 1-5 instead of the headline line")
     ap.add_argument("--shape", default="auto",
@@ -519,6 +522,60 @@ def run_config_report(args) -> None:
     print(json.dumps(out), flush=True)
 
 
+def run_sharded_bench(args) -> None:
+    """--mode sharded: one day of the headline workload split over the ranks
+    (viss_optimize_ws_b200/sharded.py; NCCL all-gather of V and gather of C),
+    timed per rank with CUDA events around the whole day (exchange included),
+    max over ranks; strong scaling."""
+    import torch
+    import viss_optimize_ws_b200 as vb
+    from viss_optimize_ws_b200 import sharded
+    ws, rank, local = dist_env()
+    dist = Dist(ws, local)
+    vb.check(vb.lib().vb_set_device(local))
+    B = vb.synthetic_sky(256, seed=1)
+    p = vb.Pipeline(vb.run_config(**workload_kwargs()))
+    p.set_sky(B)
+    p.make_baselines()
+    comp = sharded.GpuCompute(vb, p)
+    dev = torch.device("cuda", local) if ws > 1 else torch.device("cpu")
+    if ws > 1:
+        ex = sharded.TorchExchange(dist.td, dev)
+    else:
+        class _Local:
+            def all_gather(self, piece, sizes, r):
+                return piece
+
+            def gather0(self, piece, sizes, r):
+                return piece
+        ex = _Local()
+    steps = p.n_half // p.nbl
+    for _ in range(args.warmup):
+        sharded.run_day(comp, ex, rank if ws > 1 else 0, ws, steps, p.nbl, p.npix)
+    dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        sharded.run_day(comp, ex, rank if ws > 1 else 0, ws, steps, p.nbl, p.npix)
+    e1.record()
+    torch.cuda.synchronize()
+    dist.barrier()
+    t = dist.max(e0.elapsed_time(e1))
+    r = p.run()
+    terms = r["stage1_terms"] + r["stage2_terms"]
+    if rank == 0:
+        print(json.dumps({"metric": METRIC, "value": terms * args.steps / (t * 1e-3) / 1e9, "unit": UNIT,
+                          "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t / args.steps,
+                          "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+                          "dtype": "f32+f64phase", "data": "synthetic",
+                          "config": dict(WORKLOAD, parallelism=f"sharded{ws}",
+                                         note="stage 1 by time steps + all-gather of V, stage 2 by pixels + "
+                                              "gather of C; host-orchestrated exchange")}), flush=True)
+    p.close()
+    dist.close()
+
+
 def main() -> None:
     args = parse()
     if args.impl == "reference":
@@ -526,6 +583,9 @@ def main() -> None:
         return
     if args.config:
         run_config_report(args)
+        return
+    if args.mode == "sharded":
+        run_sharded_bench(args)
         return
     import viss_optimize_ws_b200 as vb
     ws, rank, local = dist_env()

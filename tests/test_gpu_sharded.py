@@ -1,0 +1,74 @@
+"""The strong-scaling split of one day (viss_optimize_ws_b200/sharded.py)
+with the real kernels: two ranks as two processes that share this GPU and
+exchange V and C over gloo on the host (their kernels never wait on each
+other); the sharded day equals the single-GPU day to FP32 summation
+rounding, with identical visible-group counts."""
+from __future__ import annotations
+
+import os
+import socket
+
+import numpy as np
+import pytest
+import torch.multiprocessing as mp
+
+from conftest import rel_err
+
+pytestmark = pytest.mark.gpu
+
+KW = dict(nside=32, orbit_model=1, nsat=8, tsteps=96, segs=3, lambda_m=30.0, occ_R_m=6371e3, cull="tilecone",
+          viss_tile_pix=1024, mirror=1, grid_res=129, bl_max_m=0.0)
+
+
+def free_port() -> int:
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _worker(rank, ws, port, q):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    import datetime
+
+    import torch
+    import torch.distributed as td
+    import viss_optimize_ws_b200 as vb
+    from viss_optimize_ws_b200 import sharded
+    try:
+        td.init_process_group("gloo", rank=rank, world_size=ws, timeout=datetime.timedelta(seconds=120))
+        with vb.Pipeline(vb.run_config(**KW)) as p:
+            p.set_sky(vb.synthetic_sky(32, seed=8))
+            p.make_baselines()
+            comp = sharded.GpuCompute(vb, p)
+            ex = sharded.TorchExchange(td, torch.device("cpu"))
+            V, Cc, W = sharded.run_day(comp, ex, rank, ws, p.n_half // p.nbl, p.nbl, p.npix)
+        q.put((rank, "ok", V, Cc, W))
+        td.destroy_process_group()
+    except Exception as e:
+        q.put((rank, "error", repr(e)[:300], None, None))
+
+
+def test_sharded_day_matches_single_gpu(gpu, vb):
+    with vb.Pipeline(vb.run_config(**KW)) as p:
+        p.set_sky(vb.synthetic_sky(32, seed=8))
+        p.make_baselines()
+        p.run()
+        V1, C1, W1 = p.get("V_half"), p.get("C"), p.get("W")
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = free_port()
+    procs = [ctx.Process(target=_worker, args=(r, 2, port, q)) for r in range(2)]
+    for pr in procs:
+        pr.start()
+    out = sorted([q.get(timeout=300) for _ in range(2)], key=lambda o: o[0])
+    for pr in procs:
+        pr.join(timeout=60)
+        if pr.is_alive():
+            pr.kill()
+    assert [o[1] for o in out] == ["ok", "ok"], out
+    _, _, V, Cc, W = out[0]
+    assert rel_err(V, V1)[0] < 1e-6 and rel_err(Cc, C1)[0] < 1e-6
+    assert np.array_equal(W, W1)
+    assert np.array_equal(out[1][2].view(np.uint32), V.view(np.uint32))
