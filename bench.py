@@ -96,7 +96,7 @@ def config_kwargs(n: int, prec: str = "fp32_fp64phase") -> dict:
 def parse() -> argparse.Namespace:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 GPU comparison run")
@@ -711,6 +711,16 @@ def main() -> None:
                 "stage2": {"kernel": "k_recon_rec", "achieved": ach2, "frac": ach2 / peak_terms,
                            "kernel_ms": k2_ms, "units_per_launch": int(s2_eval)},
                 "fp32_fma_per_s": f32.value, "fp64_fma_per_s": f64.value, "sm_clock_mhz_microbench": clk.value}
+    # the HBM side for context: DRAM bytes of the ncu capture per launch over the live kernel time
+    hbm_peak = None
+    try:
+        hbm_peak = float(json.loads((ROOT / "MEASURED_PEAKS.json").read_text())["hbm_gbs"])
+    except (OSError, ValueError, KeyError):
+        pass
+    if traffic and hbm_peak:
+        gbs = traffic / (k1_ms * 1e-3) / 1e9
+        roofline["hbm"] = {"achieved_gbs": gbs, "peak_gbs": hbm_peak, "frac": gbs / hbm_peak,
+                           "peak_source": "MEASURED_PEAKS.json (measured)"}
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
