@@ -184,6 +184,9 @@ __device__ __forceinline__ void phase_sincos(const Baseline& b, const double2 lm
       t = __fadd_rn(t, 0.5f);
       t = __fsub_rn(t, rint_magic(t));
     }
+    // angle in [0, 2 pi) as in F32X: at |uvw| ~ 2e5 this halves the C error
+    // against an angle in [-pi, pi) (measured; the phase itself is exact to ~1e-8 turns)
+    t = (t < 0.f) ? __fadd_rn(t, 1.0f) : t;
     __sincosf(__fmul_rn(t, kTwoPiF), &s, &c);
   } else if constexpr (MODE == VB_PREC_REF32) {
     float ang = raw ? fmaf(b.kw, nm1, fmaf(b.kv, f.y, b.ku * f.x))

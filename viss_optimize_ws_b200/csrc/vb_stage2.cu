@@ -340,6 +340,7 @@ __device__ __forceinline__ void recon_phase(const GroupRec& g, double ld, double
     float er = __fadd_rn(__fadd_rn(e1, e2), __fmaf_rn(g.clo, nf, e3));
     float t = __fadd_rn(fr, er);
     t = __fsub_rn(t, rn(t));
+    t = (t < 0.f) ? __fadd_rn(t, 1.0f) : t;
     __sincosf(__fmul_rn(t, kTwoPiF2), &s, &c);
   } else if constexpr (MODE == VB_PREC_REF32) {
     const float TWO_PI = 6.2831853071795864769f;
@@ -439,6 +440,7 @@ __device__ __forceinline__ void rec_term(const TermRec<MODE>& r, const RecPix& p
       t = __fadd_rn(t, 0.5f);
       t = __fsub_rn(t, rn(t));
     }
+    t = (t < 0.f) ? __fadd_rn(t, 1.0f) : t;   // angle in [0, 2 pi), as stage 1
     float s, c;
     __sincosf(__fmul_rn(t, kTwoPiF2), &s, &c);
     acc = fmaf(r.vx, c, acc);
