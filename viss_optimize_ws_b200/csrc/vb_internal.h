@@ -93,6 +93,9 @@ struct Stage2Pixels {       // pixel records already packed by the caller
   bool cones_ready = false;  // block cones already computed in this workspace
 };
 int stage2_plan(int n_half_total, int nseg, int64_t npix, const vb_stage2_opts* o, Stage2Plan* p);
+// Exact cones of the stage-2 pixel blocks into the workspace (VB_CULL_EXACT);
+// stage2_run then skips them when Stage2Pixels::cones_ready is set.
+int stage2_prepare_cones(const vb_sky* sky, const Stage2Plan& p, void* ws, size_t cap, cudaStream_t st);
 size_t stage2_workspace(const Stage2Plan& p, void* ws, size_t cap, void** slices);
 int stage2_run(const vb_sky* sky, const vb_baselines* bl, const float* V_half, int nseg, const int* seg_t0,
                const int* seg_tlen, const Stage2Plan& p, void* ws, size_t cap, float* C, uint32_t* W,

@@ -647,10 +647,13 @@ static int ensure_ready(vb_pipeline* p) {
 static int run_once(vb_pipeline* p) {
   if (p->cfg.use_graph) {
     if (!p->gexec) {
-      // eager run first (sets kernel attributes, computes stage-2 block cones)
-      VB_TRY(enqueue_stages(p));
-      VB_CUDA(cudaStreamSynchronize(p->s));
-      p->s2_cones_ready = true;
+      // the stage-2 block cones depend on the sky geometry only: computed once
+      // outside the graph, which then replays the two stages alone
+      if (!p->s2_cones_ready) {
+        vb_sky sky = sky_of(p);
+        VB_TRY(stage2_prepare_cones(&sky, p->p2, p->ws2, p->ws2_bytes, p->s));
+        p->s2_cones_ready = true;
+      }
       VB_CUDA(cudaStreamBeginCapture(p->s, cudaStreamCaptureModeThreadLocal));
       int rc = enqueue_stages(p);
       cudaGraph_t g = nullptr;

@@ -892,6 +892,13 @@ static size_t carve2(const Stage2Plan& p, void* ws, size_t cap, S2Slices* s) {
   return c.used();
 }
 
+int stage2_prepare_cones(const vb_sky* sky, const Stage2Plan& p, void* ws, size_t cap, cudaStream_t st) {
+  if (p.cull != VB_CULL_EXACT) return VB_OK;
+  S2Slices x;
+  if (!carve2(p, ws, cap, &x)) return fail(VB_ERR_NOMEM, "stage 2: workspace too small (%zu bytes)", cap);
+  return geom_exact_cones(p.block_pix, sky->l, sky->m, sky->n, p.npix, x.cones, st);
+}
+
 size_t stage2_workspace(const Stage2Plan& p, void* ws, size_t cap, void** slices) {
   S2Slices s;
   size_t r = carve2(p, ws, cap, &s);
