@@ -67,6 +67,14 @@ struct S1Args {
   unsigned* err;
 };
 
+// one staged pixel: FP64 (l, m), (n as two words, B, n - 1), FP32 (l, m, n, B);
+// interleaved so that a pixel's loads share one address with fixed offsets
+struct __align__(16) PixRec {
+  double2 lm;
+  float4 nb;
+  float4 f4;
+};
+
 struct Baseline {
   double U, V, W, C;
   float uf, vf, wf, fw;   // FP32 copies; fw = -frac(w) (raw phase, DS)
@@ -164,9 +172,10 @@ __device__ __forceinline__ void phase_sincos(const Baseline& b, const double2 lm
                                              double& sd, double& cd, bool raw) {
   if constexpr (MODE == VB_PREC_FP32_FP64PH) {
     double t = fma(b.U, lm.x, fma(b.V, lm.y, fma(b.W, nd, b.C)));
-    unsigned lo = (unsigned)__double2loint(t);
-    if constexpr (PAR) lo ^= 1u << 22;   // + 1/2 turn (top fraction bit)
-    unsigned kb = (lo & 0x7FFFFFu) | 0x4B000000u;
+    const unsigned lo = (unsigned)__double2loint(t);
+    // (lo & M) has no bits above 22: OR with the exponent bits is an XOR, and
+    // the odd pixels' half turn (bit 22) folds into the same constant
+    const unsigned kb = (lo & 0x7FFFFFu) ^ (PAR ? 0x4B400000u : 0x4B000000u);
     float ang = __fmaf_rn(__uint_as_float(kb), kAngScale, -kTwoPiF);
     __sincosf(ang, &s, &c);
   } else if constexpr (MODE == VB_PREC_FP32_DSPH) {
@@ -210,9 +219,7 @@ __device__ constexpr float imag_sign() {
 template <int MODE, int BPT, int MINB, int CULL>
 __global__ void __maxnreg__(MINB == 3 ? 80 : 120) k_stage1(const S1Args a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  double2* s_lm = reinterpret_cast<double2*>(smem_raw);
-  float4* s_nb = reinterpret_cast<float4*>(s_lm + a.stage_pix);
-  float4* s_f4 = s_nb + a.stage_pix;
+  PixRec* s_px = reinterpret_cast<PixRec*>(smem_raw);
   __shared__ int s_item;
   __shared__ unsigned long long s_cnt[4];
 
@@ -291,9 +298,11 @@ __global__ void __maxnreg__(MINB == 3 ? 80 : 120) k_stage1(const S1Args a) {
         const int ns = (int)((t1 - s0) < a.stage_pix ? (t1 - s0) : a.stage_pix);
         __syncthreads();
         for (int j = threadIdx.x; j < ns; j += S1_THREADS) {
-          s_lm[j] = a.lm[s0 + j];
-          s_nb[j] = a.nb[s0 + j];
-          s_f4[j] = a.f4[s0 + j];
+          PixRec r;
+          r.lm = a.lm[s0 + j];
+          r.nb = a.nb[s0 + j];
+          r.f4 = a.f4[s0 + j];
+          s_px[j] = r;
         }
         __syncthreads();
         if (!warp_live) continue;
@@ -315,11 +324,12 @@ __global__ void __maxnreg__(MINB == 3 ? 80 : 120) k_stage1(const S1Args a) {
           constexpr int PATH = decltype(path_tag)::value;
           constexpr bool MASKED = (PATH == 2);
           constexpr int PAR = decltype(par_tag)::value;
-          const double2 lm = s_lm[j];
-          const float4 nb = s_nb[j];
+          const PixRec* rp = s_px + j;
+          const double2 lm = rp->lm;
+          const float4 nb = rp->nb;
           const double nd = __hiloint2double(__float_as_int(nb.y), __float_as_int(nb.x));
           float4 f;
-          if constexpr (MASKED || MODE == VB_PREC_FP32_DSPH || MODE == VB_PREC_REF32) f = s_f4[j];
+          if constexpr (MASKED || MODE == VB_PREC_FP32_DSPH || MODE == VB_PREC_REF32) f = rp->f4;
           else f = make_float4(0.f, 0.f, 0.f, nb.z);
           const float Bp = nb.z;
 #pragma unroll
