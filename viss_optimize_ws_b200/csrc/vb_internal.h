@@ -97,6 +97,19 @@ int stage2_plan(int n_half_total, int nseg, int64_t npix, const vb_stage2_opts* 
 // stage2_run then skips them when Stage2Pixels::cones_ready is set.
 int stage2_prepare_cones(const vb_sky* sky, const Stage2Plan& p, void* ws, size_t cap, cudaStream_t st);
 size_t stage2_workspace(const Stage2Plan& p, void* ws, size_t cap, void** slices);
+// stage2_run in two parts: stage2_group (per-segment fit, keys, sort, group
+// starts; reads only the baselines) and stage2_finish (group records, the
+// reconstruction, finalisation).  The caller orders finish after group.
+struct Stage2Groups {
+  int sorted_keys_alt = 0;   // the sorted keys / indices sit in the second buffer of their pair
+  int sorted_vals_alt = 0;
+};
+int stage2_group(const vb_baselines* bl, int nseg, const int* seg_t0, const int* seg_tlen, const Stage2Plan& p,
+                 void* ws, size_t cap, cudaStream_t s, Stage2Groups* out);
+int stage2_finish(const vb_sky* sky, const vb_baselines* bl, const float* V_half, int nseg, const Stage2Plan& p,
+                  void* ws, size_t cap, const Stage2Groups& gr, float* C, uint32_t* W, vb_seg_params* seg_params,
+                  unsigned long long* counters, double* w_scalar_total, cudaStream_t s, const Stage2Pixels* pre,
+                  cudaEvent_t kbeg = nullptr, cudaEvent_t kend = nullptr);
 int stage2_run(const vb_sky* sky, const vb_baselines* bl, const float* V_half, int nseg, const int* seg_t0,
                const int* seg_tlen, const Stage2Plan& p, void* ws, size_t cap, float* C, uint32_t* W,
                vb_seg_params* seg_params, unsigned long long* counters, double* w_scalar_total,

@@ -128,6 +128,8 @@ struct vb_pipeline {
   unsigned long long* counters = nullptr;  // [0..3] stage 1, [4..7] stage 2
   // timing / graph
   cudaEvent_t ev[10] = {};
+  cudaStream_t s_side = nullptr;   // stage-2 grouping, concurrent with stage 1
+  cudaEvent_t fork = nullptr, join = nullptr;
   int graph_kernels = 0;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t gexec = nullptr;
@@ -184,6 +186,9 @@ static void pipeline_free(vb_pipeline* p) {
   if (p->graph) cudaGraphDestroy(p->graph);
   for (auto& e : p->ev)
     if (e) cudaEventDestroy(e);
+  if (p->fork) cudaEventDestroy(p->fork);
+  if (p->join) cudaEventDestroy(p->join);
+  if (p->s_side) cudaStreamDestroy(p->s_side);
   if (p->orb) vb_orbit_destroy(p->orb);
   for (void* q : p->owned) cudaFree(q);
   if (p->s) cudaStreamDestroy(p->s);
@@ -350,7 +355,10 @@ extern "C" int vb_pipeline_create(const vb_run_config* c, vb_pipeline** out) {
     }                                                                  \
   } while (0)
   PCUDA(cudaStreamCreateWithFlags(&p->s, cudaStreamNonBlocking));
+  PCUDA(cudaStreamCreateWithFlags(&p->s_side, cudaStreamNonBlocking));
   for (auto& e : p->ev) PCUDA(cudaEventCreate(&e));
+  PCUDA(cudaEventCreateWithFlags(&p->fork, cudaEventDisableTiming));
+  PCUDA(cudaEventCreateWithFlags(&p->join, cudaEventDisableTiming));
 
   // physics: global horizon cosine of the upstream lunar set-up (main_recon_online.cu:83-86)
   {
@@ -517,22 +525,39 @@ extern "C" int vb_pipeline_make_baselines(vb_pipeline* p) {
   return VB_OK;
 }
 
-// Both stages on p->s (capturable).
+// Both stages from p->s (capturable).  Stage 2's grouping reads only the
+// baselines, so it runs on p->s_side, forked from p->s before stage 1 and
+// joined before the rest of stage 2: its short kernels fill SMs that stage 1's
+// persistent CTAs leave free, mostly in stage 1's tail.
 static int enqueue_stages(vb_pipeline* p) {
   vb_sky sky = sky_of(p);
   vb_baselines bl = bl_of(p);
   VB_CUDA(cudaMemsetAsync(p->counters, 0, 8 * sizeof(unsigned long long), p->s));
   VB_CUDA(record_event(p->ev[0], p->s));
-  VB_TRY(stage1_run(&sky, &bl, p->p1, p->b1, true, p->Vd, p->counters, p->s, p->ev[5], p->ev[6]));
-  VB_TRY(phase_correct_expand_async(p->Vd, p->w, p->n_half, p->nbl, 1, p->Vh, p->Vf, p->s));
-  VB_CUDA(record_event(p->ev[1], p->s));
+  VB_CUDA(cudaEventRecord(p->fork, p->s));
+  VB_CUDA(cudaStreamWaitEvent(p->s_side, p->fork, 0));
+  Stage2Groups gr;
+  // the side stream is joined back on every path, so that a failed step never
+  // leaves it forked from a stream capture
+  int rc = stage2_group(&bl, p->nseg, p->d_t0, p->d_tlen, p->p2, p->ws2, p->ws2_bytes, p->s_side, &gr);
+  const cudaError_t ej = cudaEventRecord(p->join, p->s_side);
+  if (rc == VB_OK)
+    rc = stage1_run(&sky, &bl, p->p1, p->b1, true, p->Vd, p->counters, p->s, p->ev[5], p->ev[6]);
+  if (rc == VB_OK) rc = phase_correct_expand_async(p->Vd, p->w, p->n_half, p->nbl, 1, p->Vh, p->Vf, p->s);
+  if (rc == VB_OK) {
+    const cudaError_t e1 = record_event(p->ev[1], p->s);
+    if (e1 != cudaSuccess) rc = cuda_fail(e1, "record_event", __FILE__, __LINE__);
+  }
+  const cudaError_t ew = (ej == cudaSuccess) ? cudaStreamWaitEvent(p->s, p->join, 0) : ej;
+  if (rc != VB_OK) return rc;
+  VB_CUDA(ew);
   Stage2Pixels pre;
   pre.lm = p->b1.lm;
   pre.nb = p->b1.nb;
   pre.f4 = p->b1.f4;
   pre.cones_ready = p->s2_cones_ready;
-  VB_TRY(stage2_run(&sky, &bl, p->Vh, p->nseg, p->d_t0, p->d_tlen, p->p2, p->ws2, p->ws2_bytes, p->C, p->W,
-                    p->segp, p->counters + 4, p->wsum, p->s, &pre, p->ev[7], p->ev[8]));
+  VB_TRY(stage2_finish(&sky, &bl, p->Vh, p->nseg, p->p2, p->ws2, p->ws2_bytes, gr, p->C, p->W, p->segp,
+                       p->counters + 4, p->wsum, p->s, &pre, p->ev[7], p->ev[8]));
   VB_CUDA(record_event(p->ev[2], p->s));
   return VB_OK;
 }

@@ -937,14 +937,17 @@ __global__ void k_expand_half(const float* __restrict__ Vh, int n_half, int nbl,
   }
 }
 
-int stage2_run(const vb_sky* sky, const vb_baselines* bl, const float* V_half, int nseg, const int* seg_t0,
-               const int* seg_tlen, const Stage2Plan& p, void* ws, size_t cap, float* C, uint32_t* W,
-               vb_seg_params* seg_params_out, unsigned long long* counters, double* w_scalar_total, cudaStream_t st,
-               const Stage2Pixels* pre, cudaEvent_t kbeg, cudaEvent_t kend) {
+// Steps 1-4 read only the baselines (u, v and the segment table), so a caller
+// may run them on a second stream concurrently with stage 1; the sort's
+// double-buffer choice is known at enqueue time and handed to stage2_finish.
+int stage2_group(const vb_baselines* bl, int nseg, const int* seg_t0, const int* seg_tlen, const Stage2Plan& p,
+                 void* ws, size_t cap, cudaStream_t st, Stage2Groups* out) {
   S2Slices x;
   if (!carve2(p, ws, cap, &x)) return fail(VB_ERR_NOMEM, "stage 2: workspace too small (%zu bytes)", cap);
   const int n = p.n_keyed_total;
   const int nbl = bl->nbl;
+  out->sorted_keys_alt = 0;
+  out->sorted_vals_alt = 0;
   VB_CUDA(cudaMemsetAsync(x.err, 0, sizeof(unsigned), st));
   VB_CUDA(cudaMemsetAsync(x.ngroups, 0, sizeof(int), st));
   VB_CUDA(cudaMemsetAsync(x.wsum, 0, sizeof(double), st));
@@ -954,8 +957,6 @@ int stage2_run(const vb_sky* sky, const vb_baselines* bl, const float* V_half, i
   k_seg_fit<<<nseg, 256, 0, st>>>(bl->u, bl->v, bl->w, nbl, seg_t0, seg_tlen, p.bl_max, p.lambda, p.grid_res,
                                   p.mirror, x.sp);
   VB_LAUNCH_CHECK();
-  const int* sv = nullptr;
-  const float* Vk = V_half;
   if (n > 0) {
     // 2. keys
     k_keys<<<g, 256, 0, st>>>(bl->u, bl->v, n, nbl, p.mirror, seg_t0, nseg, x.sp, x.k0, x.v0, nullptr);
@@ -968,7 +969,8 @@ int stage2_run(const vb_sky* sky, const vb_baselines* bl, const float* V_half, i
     size_t sb = p.cub_sort_bytes;
     VB_CUDA(cub::DeviceRadixSort::SortPairs(x.cub_sort, sb, dk, dv, n, 0, 32 + seg_bits, st));
     const unsigned long long* sk = dk.Current();
-    sv = dv.Current();
+    out->sorted_keys_alt = dk.selector;
+    out->sorted_vals_alt = dv.selector;
     // 4. runs -> groups
     k_run_flags<<<g, 256, 0, st>>>(sk, n, x.flags);
     VB_LAUNCH_CHECK();
@@ -976,6 +978,26 @@ int stage2_run(const vb_sky* sky, const vb_baselines* bl, const float* V_half, i
     VB_CUDA(cub::DeviceScan::InclusiveSum(x.cub_scan, scb, x.flags, x.gid, n, st));
     k_group_starts<<<g, 256, 0, st>>>(x.flags, x.gid, n, sk, x.start, x.ngroups, x.sp);
     VB_LAUNCH_CHECK();
+  }
+  return VB_OK;
+}
+
+// Steps 5-9, after stage2_group (same workspace, ordered after it on st).
+int stage2_finish(const vb_sky* sky, const vb_baselines* bl, const float* V_half, int nseg, const Stage2Plan& p,
+                  void* ws, size_t cap, const Stage2Groups& gr, float* C, uint32_t* W, vb_seg_params* seg_params_out,
+                  unsigned long long* counters, double* w_scalar_total, cudaStream_t st, const Stage2Pixels* pre,
+                  cudaEvent_t kbeg, cudaEvent_t kend) {
+  S2Slices x;
+  if (!carve2(p, ws, cap, &x)) return fail(VB_ERR_NOMEM, "stage 2: workspace too small (%zu bytes)", cap);
+  const int n = p.n_keyed_total;
+  const int nbl = bl->nbl;
+  int g = (int)ceil_div(n > 0 ? n : 1, 256);
+  if (g > sm_count() * 16) g = sm_count() * 16;
+  const int* sv = nullptr;
+  const float* Vk = V_half;
+  if (n > 0) {
+    const unsigned long long* sk = gr.sorted_keys_alt ? x.k1 : x.k0;
+    sv = gr.sorted_vals_alt ? x.v1 : x.v0;
     // 5. V in the keyed layout (full grid: conjugate-completed signed set)
     if (!p.mirror) {
       k_expand_half<<<g, 256, 0, st>>>(V_half, p.n_half_total, nbl, x.Vfull);
@@ -1040,6 +1062,16 @@ int stage2_run(const vb_sky* sky, const vb_baselines* bl, const float* V_half, i
     VB_CUDA(cudaMemcpyAsync(seg_params_out, x.sp, nseg * sizeof(vb_seg_params), cudaMemcpyDeviceToDevice, st));
   if (w_scalar_total) VB_CUDA(cudaMemcpyAsync(w_scalar_total, x.wsum, sizeof(double), cudaMemcpyDeviceToDevice, st));
   return VB_OK;
+}
+
+int stage2_run(const vb_sky* sky, const vb_baselines* bl, const float* V_half, int nseg, const int* seg_t0,
+               const int* seg_tlen, const Stage2Plan& p, void* ws, size_t cap, float* C, uint32_t* W,
+               vb_seg_params* seg_params_out, unsigned long long* counters, double* w_scalar_total, cudaStream_t st,
+               const Stage2Pixels* pre, cudaEvent_t kbeg, cudaEvent_t kend) {
+  Stage2Groups gr;
+  VB_TRY(stage2_group(bl, nseg, seg_t0, seg_tlen, p, ws, cap, st, &gr));
+  return stage2_finish(sky, bl, V_half, nseg, p, ws, cap, gr, C, W, seg_params_out, counters, w_scalar_total, st,
+                       pre, kbeg, kend);
 }
 
 }  // namespace vb
