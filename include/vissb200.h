@@ -210,9 +210,10 @@ int vb_viss_halfsym(const vb_sky* sky, const vb_baselines* bl,
 /* Largest scratch of vb_viss_halfsym_noalloc, in bytes (64 MiB). */
 #define VB_VISS_NOALLOC_MAX_BYTES (64u << 20)
 
-/* vb_viss_halfsym for callers that cannot allocate device memory: code that
- * runs while a stream is being captured into a CUDA graph, hosts whose device
- * memory belongs to another allocator with a fixed budget, real-time loops.
+/* vb_viss_halfsym for callers that cannot allocate device memory: hosts whose
+ * device memory belongs to another allocator with a fixed budget, and
+ * real-time loops that cannot afford the latency and implicit device
+ * synchronisation of cudaMalloc / cudaFree.
  * The caller passes only inputs and outputs.  No counterpart in the upstream
  * project (upstream allocates everything in main()).
  * Scratch is one file-scope device array of VB_VISS_NOALLOC_MAX_BYTES that

@@ -1,6 +1,7 @@
 """vb_viss_halfsym_noalloc -- the stage-1 visibility sum for callers that
-cannot allocate device memory (code inside a CUDA stream capture, hosts whose
-device memory belongs to another allocator, real-time loops) -- against the
+cannot allocate device memory (hosts whose device memory belongs to another
+allocator with a fixed budget, real-time loops that cannot afford the latency
+and synchronisation of cudaMalloc) -- against the
 workspace entry point vb_viss_halfsym, through the C ABI, on two calls in a
 row; and its clear error above the fixed scratch maximum.
 

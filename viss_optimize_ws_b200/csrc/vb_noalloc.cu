@@ -2,12 +2,13 @@
 //
 // vb_viss_halfsym needs scratch (packed pixel records, per-chunk partial
 // sums, a work counter) that its caller allocates.  Some callers cannot call
-// cudaMalloc at all: code that runs while a stream is being captured into a
-// CUDA graph (allocation is illegal there), plug-in hosts whose device memory
-// is owned by another allocator with a fixed budget, and real-time loops that
-// must not pay allocation latency.  This entry point takes only its inputs and
-// outputs and keeps its scratch in one file-scope device array of fixed
-// maximum size, which every GPU that loads the library holds until exit.
+// cudaMalloc at all: plug-in hosts whose device memory is owned by another
+// allocator with a fixed budget (a cudaMalloc behind its back can fail or
+// break its accounting), and real-time loops that must not pay the latency
+// and implicit device synchronisation of cudaMalloc / cudaFree.  This entry
+// point takes only its inputs and outputs and keeps its scratch in one
+// file-scope device array of fixed maximum size, which every GPU that loads
+// the library holds until exit.
 #include <mutex>
 
 #include "vb_common.cuh"
