@@ -762,7 +762,7 @@ static int run_slabs(vb_pipeline* p, const float* B_host, int scale, float* C_ho
     }
     vb_sky sky = sky_of(p);
     sky.npix = cnt;
-    Stage1Plan q;
+    Stage1Plan q{};
     VB_TRY(stage1_plan(&sky, &bl, &o1, &q));
     Stage1Buffers b;
     if (!stage1_carve(q, p->ws1, p->ws1_bytes, &b, true))
@@ -789,7 +789,7 @@ static int run_slabs(vb_pipeline* p, const float* B_host, int scale, float* C_ho
     VB_TRY(slab_geometry(p, base, cnt));
     vb_sky sky = sky_of(p);
     sky.npix = cnt;
-    Stage2Plan q;
+    Stage2Plan q{};
     VB_TRY(stage2_plan(p->n_half, p->nseg, cnt, &o2, &q));
     VB_TRY(stage2_run(&sky, &bl, p->Vh, p->nseg, p->d_t0, p->d_tlen, q, p->ws2, p->ws2_bytes, p->C, p->W, p->segp,
                       p->counters + 4, p->wsum, p->s, nullptr));

@@ -703,14 +703,14 @@ int phase_correct_expand_async(const double* Vraw, const float* w_full, int n_ha
 using namespace vb;
 
 extern "C" size_t vb_stage1_workspace_bytes(const vb_sky* sky, const vb_baselines* bl, const vb_stage1_opts* o) {
-  Stage1Plan p;
+  Stage1Plan p{};
   if (stage1_plan(sky, bl, o, &p) != VB_OK) return 0;
   return stage1_carve(p, nullptr, 0, nullptr, true);
 }
 
 extern "C" int vb_viss_halfsym(const vb_sky* sky, const vb_baselines* bl, const vb_stage1_opts* o, void* workspace,
                                size_t ws_bytes, double* V_half, unsigned long long* term_counters, void* stream) {
-  Stage1Plan p;
+  Stage1Plan p{};
   VB_TRY(stage1_plan(sky, bl, o, &p));
   if (p.n_half == 0) return VB_OK;
   if (!V_half) return fail(VB_ERR_INVALID, "vb_viss_halfsym: V_half is NULL");
@@ -754,7 +754,7 @@ __global__ void k_tile_classes(const S1Args a, int ntile, uint8_t* __restrict__ 
 
 extern "C" int vb_stage1_tile_classes(const vb_sky* sky, const vb_baselines* bl, const vb_stage1_opts* o,
                                       void* workspace, size_t ws_bytes, uint8_t* cls, int* ntile_out, void* stream) {
-  Stage1Plan p;
+  Stage1Plan p{};
   VB_TRY(stage1_plan(sky, bl, o, &p));
   if (ntile_out) *ntile_out = p.ntile_cull;
   if (p.n_half == 0) return VB_OK;

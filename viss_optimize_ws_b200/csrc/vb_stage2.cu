@@ -1154,7 +1154,7 @@ extern "C" int vb_build_keys(const float* u_full, const float* v_full, int n, in
 }
 
 extern "C" size_t vb_stage2_workspace_bytes(int n_half_total, int nseg, int64_t npix, const vb_stage2_opts* o) {
-  Stage2Plan p;
+  Stage2Plan p{};
   if (stage2_plan(n_half_total, nseg, npix, o, &p) != VB_OK) return 0;
   return stage2_workspace(p, nullptr, 0, nullptr);
 }
@@ -1166,7 +1166,7 @@ extern "C" int vb_recon_batched(const vb_sky* sky, const vb_baselines* bl, const
   if (!sky || !bl || !o) return fail(VB_ERR_INVALID, "vb_recon_batched: null argument");
   if (bl->nbl <= 0 || bl->n_full % (2 * bl->nbl) != 0) return fail(VB_ERR_INVALID, "vb_recon_batched: n_full/nbl");
   if (!C || !V_half || !seg_t0 || !seg_tlen) return fail(VB_ERR_INVALID, "vb_recon_batched: null buffer");
-  Stage2Plan p;
+  Stage2Plan p{};
   VB_TRY(stage2_plan(bl->n_full / 2, nseg, sky->npix, o, &p));
   size_t need = stage2_workspace(p, nullptr, 0, nullptr);
   if (!workspace || ws_bytes < need) return fail(VB_ERR_NOMEM, "vb_recon_batched: workspace %zu < %zu", ws_bytes, need);
