@@ -2,7 +2,8 @@
 with the real kernels: two ranks as two processes that share this GPU and
 exchange V and C over gloo on the host (their kernels never wait on each
 other); the sharded day equals the single-GPU day to FP32 summation
-rounding, with identical visible-group counts."""
+rounding, with identical visible-group counts.  A second test runs the day as
+one rank over NCCL with device tensors, the exchange a multi-GPU run uses."""
 from __future__ import annotations
 
 import os
@@ -50,6 +51,34 @@ def _worker(rank, ws, port, q):
         q.put((rank, "error", repr(e)[:300], None, None))
 
 
+def _worker_nccl(port, q):
+    """One rank over NCCL with device tensors: the exchange path a multi-GPU
+    run takes, on the one GPU this test has (a one-rank all-gather is a copy)."""
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), NCCL_NVLS_ENABLE="0")
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    import datetime
+
+    import torch
+    import torch.distributed as td
+    import viss_optimize_ws_b200 as vb
+    from viss_optimize_ws_b200 import sharded
+    try:
+        torch.cuda.set_device(0)
+        td.init_process_group("nccl", rank=0, world_size=1, timeout=datetime.timedelta(seconds=120),
+                              device_id=torch.device("cuda", 0))
+        with vb.Pipeline(vb.run_config(**KW)) as p:
+            p.set_sky(vb.synthetic_sky(32, seed=8))
+            p.make_baselines()
+            comp = sharded.GpuCompute(vb, p)
+            ex = sharded.TorchExchange(td, torch.device("cuda", 0))
+            V, Cc, W = sharded.run_day(comp, ex, 0, 1, p.n_half // p.nbl, p.nbl, p.npix)
+        td.destroy_process_group()
+        q.put(("ok", V, Cc, W))
+    except Exception as e:
+        q.put(("error", repr(e)[:300], None, None))
+
+
 def test_sharded_day_matches_single_gpu(gpu, vb):
     with vb.Pipeline(vb.run_config(**KW)) as p:
         p.set_sky(vb.synthetic_sky(32, seed=8))
@@ -72,3 +101,23 @@ def test_sharded_day_matches_single_gpu(gpu, vb):
     assert rel_err(V, V1)[0] < 1e-6 and rel_err(Cc, C1)[0] < 1e-6
     assert np.array_equal(W, W1)
     assert np.array_equal(out[1][2].view(np.uint32), V.view(np.uint32))
+
+
+def test_sharded_day_over_nccl_one_rank(gpu, vb):
+    with vb.Pipeline(vb.run_config(**KW)) as p:
+        p.set_sky(vb.synthetic_sky(32, seed=8))
+        p.make_baselines()
+        p.run()
+        V1, C1, W1 = p.get("V_half"), p.get("C"), p.get("W")
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    pr = ctx.Process(target=_worker_nccl, args=(free_port(), q))
+    pr.start()
+    out = q.get(timeout=300)
+    pr.join(timeout=60)
+    if pr.is_alive():
+        pr.kill()
+    assert out[0] == "ok", out
+    _, V, Cc, W = out
+    assert rel_err(V, V1)[0] < 1e-6 and rel_err(Cc, C1)[0] < 1e-6
+    assert np.array_equal(W, W1)
