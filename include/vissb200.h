@@ -191,6 +191,10 @@ typedef struct {
   int refine_pix;       /* tile-cone culling: inside mixed tiles, exact sub-tiles of this many
                            pixels skip or drop the per-pixel test where they can (0 = 128,
                            < 0 = off); results are identical either way */
+  int mask_visible_tiles; /* tile-cone culling: 0 = tiles the cone test proves visible skip the
+                           per-pixel test (upstream's all-visible nm1 fast path,
+                           ..._vissfast.cuh:530-539); 1 = they take it like mixed tiles, so
+                           only tiles proven hidden are culled */
 } vb_stage1_opts;
 
 size_t vb_stage1_workspace_bytes(const vb_sky* sky, const vb_baselines* bl,
@@ -350,6 +354,8 @@ typedef struct {
                               vb_pipeline_run_host.  0: the whole sky is resident */
   int      use_graph;      /* 1: capture stages in one CUDA graph */
   int      device;         /* CUDA device ordinal */
+  int      nm1_fast;       /* 1 (default): upstream all-visible fast path; 0: visible tiles take the
+                              per-pixel test (vb_stage1_opts.mask_visible_tiles = 1) */
 } vb_run_config;
 
 typedef struct {

@@ -136,9 +136,10 @@ def stage1(sky, bls, *, precision, cull, phase_corrected=1, blockage=1, bpt=0, s
     return get(V, np.float64), get(cnt, np.uint64)
 
 
-def tile_classes(sky, bls, *, cull, precision=vb.PREC_FP32_FP64PH, exact_tile_pix=0, blockage=1):
+def tile_classes(sky, bls, *, cull, precision=vb.PREC_FP32_FP64PH, exact_tile_pix=0, blockage=1,
+                 mask_visible_tiles=0):
     o = vb.Stage1Opts(precision=precision, cull=cull, phase_corrected=1, blockage=blockage,
-                      exact_tile_pix=exact_tile_pix)
+                      exact_tile_pix=exact_tile_pix, mask_visible_tiles=mask_visible_tiles)
     need = vb.lib().vb_stage1_workspace_bytes(C.byref(sky), C.byref(bls), C.byref(o))
     ws = DeviceBuffer(need)
     nt = C.c_int()

@@ -43,7 +43,7 @@ def pipeline_tile_classes(vb, p):
     c1, n1 = p.ptr("cosphi1")
     if c1 and n1:                                   # per-endpoint horizon cosines
         bl.cosphi1, bl.cosphi2 = c1, p.ptr("cosphi2")[0]
-    cls, tile = tile_classes(sky, bl, cull=vb.CULL_TILECONE)
+    cls, tile = tile_classes(sky, bl, cull=vb.CULL_TILECONE, mask_visible_tiles=0 if p.cfg.nm1_fast else 1)
     return cls, tile
 
 
@@ -81,6 +81,33 @@ def test_pipeline_vs_oracle(gpu, vb, orc, model):
         assert emax <= TOL and erms <= TOL, (emax, erms)
         assert rep["stage1_terms"] == p.npix * p.n_half
         assert rep["stage2_terms"] == p.npix * sum(s["nuniq"] for s in sp)
+
+
+def test_nm1_fast_off_vs_oracle(gpu, vb, orc):
+    """--nm1_fast=0: tiles the cone test proves visible take the per-pixel test
+    like mixed tiles (upstream's all-visible fast path, ..._vissfast.cuh:530-539,
+    switched off); only tiles proven hidden are culled.  Against the oracle
+    with the same tile classes, and against the default where they differ."""
+    kw = dict(nside=16, orbit_model=vb.ORBIT_SYNTHETIC, nsat=8, tsteps=64, segs=4, lambda_m=30.0,
+              occ_R_m=6371e3, cull="tilecone", viss_tile_pix=256, mirror=1, grid_res=129, bl_max_m=100e3)
+    B = vb.synthetic_sky(16, seed=2)
+    res = {}
+    for fast in (1, 0):
+        with vb.Pipeline(vb.run_config(nm1_fast=fast, **kw)) as p:
+            p.set_sky(B)
+            p.make_baselines()
+            rep = p.run()
+            assert rep["error_flags"] == 0
+            cls, tile = pipeline_tile_classes(vb, p)
+            res[fast] = (p.get("V_half"), cls, rep["s1_counters"])
+            if not fast:
+                sky, bl = host_inputs(p)
+                Vo = orc.stage1(sky, bl, phase_corrected=1, tile_pix=tile, tile_cls=cls, precision=1)
+                emax, erms = rel_err(res[0][0], Vo)
+                assert emax <= TOL and erms <= TOL, (emax, erms)
+    assert np.any(res[1][1] == 1) and not np.any(res[0][1] == 1)       # no tile is taken as visible
+    assert np.array_equal(res[1][1] == 0, res[0][1] == 0)               # the same tiles are culled
+    assert res[0][2][3] == res[1][2][3] and res[0][2][2] >= res[1][2][2]  # same nominal terms, no fewer skipped
 
 
 def test_graph_eager_determinism_and_host_entry(gpu, vb):

@@ -44,7 +44,8 @@ class Baselines(C.Structure):
 class Stage1Opts(C.Structure):
     _fields_ = [("precision", C.c_int), ("cull", C.c_int), ("phase_corrected", C.c_int), ("blockage", C.c_int),
                 ("bpt", C.c_int), ("stage_pix", C.c_int), ("chunk_pix", C.c_int), ("exact_tile_pix", C.c_int),
-                ("ctas_per_sm", C.c_int), ("items_per_cta", C.c_int), ("refine_pix", C.c_int)]
+                ("ctas_per_sm", C.c_int), ("items_per_cta", C.c_int), ("refine_pix", C.c_int),
+                ("mask_visible_tiles", C.c_int)]
 
 
 class Stage2Opts(C.Structure):
@@ -75,7 +76,8 @@ class RunConfig(C.Structure):
                 ("seg_min_half", C.c_int), ("seg_max_half", C.c_int), ("seg_seed", C.c_uint64),
                 ("stage2_cull", C.c_int), ("stage2_ppt", C.c_int), ("stage2_items_per_cta", C.c_int),
                 ("stage1_bpt", C.c_int), ("stage1_stage_pix", C.c_int), ("stage1_ctas_per_sm", C.c_int),
-                ("stage1_items_per_cta", C.c_int), ("stage1_refine_pix", C.c_int), ("slab_pix", C.c_int64), ("use_graph", C.c_int), ("device", C.c_int)]
+                ("stage1_items_per_cta", C.c_int), ("stage1_refine_pix", C.c_int), ("slab_pix", C.c_int64), ("use_graph", C.c_int), ("device", C.c_int),
+                ("nm1_fast", C.c_int)]
 
 
 class Report(C.Structure):

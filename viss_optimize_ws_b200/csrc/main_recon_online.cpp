@@ -169,6 +169,9 @@ int main(int argc, char** argv) {
   // additive flags (this build)
   int mirror = to_int(get_arg(argc, argv, "--mirror", vissfast ? "1" : "0"), vissfast ? 1 : 0);
   int tilecone = to_int(get_arg(argc, argv, "--tilecone", vissfast ? "1" : "0"), vissfast ? 1 : 0);
+  // 1: tiles the cone test proves visible skip the per-pixel test (the upstream
+  // all-visible nm1 fast path); 0: they take it, only hidden tiles are culled
+  int nm1_fast = to_int(get_arg(argc, argv, "--nm1_fast", "1"), 1);
   std::string prec_s = get_arg(argc, argv, "--precision", "fp32_fp64phase");
   std::string orbit_model = get_arg(argc, argv, "--orbit_model", "reference");
   int nsat = to_int(get_arg(argc, argv, "--nsat", "8"), 8);
@@ -288,6 +291,7 @@ int main(int argc, char** argv) {
   cfg.seg_max_half = seg_max;
   cfg.seg_seed = seg_seed;
   cfg.stage2_cull = stage2_cull;
+  cfg.nm1_fast = nm1_fast ? 1 : 0;
   cfg.slab_pix = slab_pix;
   cfg.use_graph = use_graph;
   cfg.device = 0;

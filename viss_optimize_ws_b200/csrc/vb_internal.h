@@ -46,6 +46,7 @@ int geom_invnorm(const float* x, const float* y, const float* z, float* invn, in
 struct Stage1Plan {
   int precision, cull, phase_corrected, blockage;
   int bpt, minb, stage_pix, chunk_pix, cull_tile, refine_pix;
+  int mask_visible;   // tile-cone: tiles proven visible still take the per-pixel test
   int64_t npix;
   int n_half, nbl;
   int nchunk, n_btile, n_items, grid;

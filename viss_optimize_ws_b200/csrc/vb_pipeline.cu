@@ -167,6 +167,7 @@ extern "C" void vb_run_config_defaults(vb_run_config* c) {
   c->stage2_cull = VB_CULL_EXACT;
   c->use_graph = 1;
   c->device = 0;
+  c->nm1_fast = 1;
 }
 
 template <class T>
@@ -587,6 +588,7 @@ static int plan_stages(vb_pipeline* p) {
   o1.ctas_per_sm = c->stage1_ctas_per_sm;
   o1.items_per_cta = c->stage1_items_per_cta;
   o1.refine_pix = c->stage1_refine_pix;
+  o1.mask_visible_tiles = c->nm1_fast ? 0 : 1;
   Stage1Plan p1;
   VB_TRY(stage1_plan(&sky, &bl, &o1, &p1));
   vb_stage2_opts o2{};
@@ -749,6 +751,7 @@ static int run_slabs(vb_pipeline* p, const float* B_host, int scale, float* C_ho
   o1.ctas_per_sm = p->cfg.stage1_ctas_per_sm;
   o1.items_per_cta = p->cfg.stage1_items_per_cta;
   o1.refine_pix = p->cfg.stage1_refine_pix;
+  o1.mask_visible_tiles = p->cfg.nm1_fast ? 0 : 1;
   VB_CUDA(record_event(p->ev[0], p->s));
   for (int k = 0; k < p->nslab; ++k) {
     const int64_t base = (int64_t)k * p->nres;

@@ -58,6 +58,7 @@ struct S1Args {
   const ExactCone* cones;                          // VB_CULL_EXACT
   const ExactCone* subcones;                       // tile-cone refinement: cones of refine_pix sub-tiles
   int refine_pix;                                  // 0: no refinement
+  int mask_visible;                                // tile-cone: visible tiles take the per-pixel test
   const float *u, *v, *w, *x1, *y1, *z1, *in1, *x2, *y2, *z2, *in2, *cp1, *cp2;
   float cosphi;
   int n_half, nbl, blockage, phase_corrected;
@@ -116,7 +117,7 @@ __device__ __forceinline__ int tile_class(const S1Args& a, const Baseline& b, in
     bool vis1, hid1, vis2, hid2;
     cone_classify(cone_dot(b.ux1, b.uy1, b.uz1, cx, cy, cz), cA, sA, b.c1, vis1, hid1);
     cone_classify(cone_dot(b.ux2, b.uy2, b.uz2, cx, cy, cz), cA, sA, b.c2, vis2, hid2);
-    return (hid1 || hid2) ? kClsHid : ((vis1 && vis2) ? kClsVis : kClsMix);
+    return (hid1 || hid2) ? kClsHid : ((vis1 && vis2 && !a.mask_visible) ? kClsVis : kClsMix);
   } else if constexpr (CULL == VB_CULL_EXACT) {
     return exact_tile_class(a.cones + tile_id, b.x1, b.y1, b.z1, b.i1, b.c1, b.x2, b.y2, b.z2, b.i2, b.c2);
   } else {
@@ -592,6 +593,7 @@ int stage1_plan(const vb_sky* sky, const vb_baselines* bl, const vb_stage1_opts*
   // on the nside-256 workload 128-pixel sub-tiles cut the masked terms from
   // 2.77e9 to 1.44e9 and the kernel time by 6 %)
   q.refine_pix = 0;
+  q.mask_visible = (q.cull == VB_CULL_TILECONE && o->mask_visible_tiles) ? 1 : 0;
   if (q.cull == VB_CULL_TILECONE && o->refine_pix >= 0) {
     int r = o->refine_pix > 0 ? o->refine_pix : 128;
     if (!is_pow2(r) || r < 32) return fail(VB_ERR_INVALID, "stage 1: refine_pix=%d (power of two >= 32)", r);
@@ -667,6 +669,7 @@ int stage1_run(const vb_sky* sky, const vb_baselines* bl, const Stage1Plan& p, c
   a.cones = b.cones;
   a.subcones = b.subcones;
   a.refine_pix = p.refine_pix;
+  a.mask_visible = p.mask_visible;
   a.u = bl->u; a.v = bl->v; a.w = bl->w;
   a.x1 = bl->x1; a.y1 = bl->y1; a.z1 = bl->z1; a.in1 = bl->invn1;
   a.x2 = bl->x2; a.y2 = bl->y2; a.z2 = bl->z2; a.in2 = bl->invn2;
@@ -777,6 +780,7 @@ extern "C" int vb_stage1_tile_classes(const vb_sky* sky, const vb_baselines* bl,
   a.x2 = bl->x2; a.y2 = bl->y2; a.z2 = bl->z2; a.in2 = bl->invn2;
   a.cp1 = bl->cosphi1; a.cp2 = bl->cosphi2; a.cosphi = bl->cosphi;
   a.n_half = p.n_half; a.nbl = p.nbl; a.blockage = p.blockage; a.phase_corrected = p.phase_corrected;
+  a.mask_visible = p.mask_visible;
   int64_t total = (int64_t)p.n_half * p.ntile_cull;
   int g = (int)std::min<int64_t>(ceil_div(total, 256), (int64_t)sm_count() * 16);
   k_tile_classes<<<g, 256, 0, s>>>(a, p.ntile_cull, cls);
