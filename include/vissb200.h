@@ -311,10 +311,20 @@ int vb_recon_batched(const vb_sky* sky, const vb_baselines* bl, const float* V_h
                      float* C, uint32_t* W, vb_seg_params* seg_params,
                      unsigned long long* term_counters, void* stream);
 
+/* Short names for the two stage kernels: vb_stage1 is vb_viss_halfsym without
+ * the term counters, vb_stage2 is vb_recon_batched without seg_params and the
+ * term counters.  Same upstream kernels replaced as those two entries. */
+int vb_stage1(const vb_sky* sky, const vb_baselines* bl, const vb_stage1_opts* o,
+              void* workspace, size_t ws_bytes, double* V_half, void* stream);
+int vb_stage2(const vb_sky* sky, const vb_baselines* bl, const float* V_half,
+              int nseg, const int* seg_t0, const int* seg_tlen, const vb_stage2_opts* o,
+              void* workspace, size_t ws_bytes, float* C, uint32_t* W, void* stream);
+
 /* ------------------------------------------------------------------------ */
 /* whole pipeline (the main_recon_online run)                                */
 /* ------------------------------------------------------------------------ */
 typedef struct vb_pipeline vb_pipeline;
+
 
 typedef struct {
   /* upstream flags (main_recon_online.cu:6-27, ..._mirror_tile_vissfast.cu:7-31) */
@@ -405,6 +415,17 @@ int vb_pipeline_run(vb_pipeline* p, vb_report* r);
  * C_host (npix floats) and, if non-NULL, V_half_host (2*n_half floats) back. */
 int vb_pipeline_run_host(vb_pipeline* p, const float* B_host, int scale,
                          float* C_host, float* V_half_host, vb_report* r);
+
+/* One whole run in one call, as upstream main() does for one day
+ * (main_recon_online.cu:5-586 without the file IO): builds a pipeline from c,
+ * uploads B_host (npix floats, scaled by 4 pi / npix when scale is set),
+ * generates the day's baselines, runs both stages, copies C (npix floats)
+ * and, if V_half_host is non-NULL, the phase-corrected half-set V
+ * (2 * n_half floats) back, and frees everything.  r (nullable) receives the
+ * run's report.  npix_expected must equal 12 * nside^2 (a size check of the
+ * caller's buffers). */
+int vb_run(const vb_run_config* c, const float* B_host, int scale, int64_t npix_expected,
+           float* C_host, float* V_half_host, vb_report* r);
 
 /* Device pointers owned by the pipeline (valid until destroy), for tests and
  * writers.  name: "C","W","V_half","V_full","V_half_d","u","v","w","x1","y1","z1",

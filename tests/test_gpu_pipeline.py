@@ -110,6 +110,64 @@ def test_nm1_fast_off_vs_oracle(gpu, vb, orc):
     assert res[0][2][3] == res[1][2][3] and res[0][2][2] >= res[1][2][2]  # same nominal terms, no fewer skipped
 
 
+def test_one_call_run_and_stage_names(gpu, vb):
+    """vb_run (one call: create, upload, baselines, both stages, download,
+    free) equals the pipeline's host entry bit for bit and rejects a wrong
+    buffer size; vb_stage1 / vb_stage2 equal vb_viss_halfsym /
+    vb_recon_batched on the pipeline's own device arrays."""
+    from gpu_util import DeviceBuffer, dev, get, zeros
+    cfg = vb.run_config(nside=16, orbit_model=vb.ORBIT_SYNTHETIC, nsat=8, tsteps=32, segs=2, lambda_m=30.0,
+                        occ_R_m=6371e3, cull="tilecone", viss_tile_pix=256, mirror=1, grid_res=65, bl_max_m=100e3)
+    B = vb.synthetic_sky(16, seed=5)
+    with vb.Pipeline(cfg) as p:
+        C1, V1, _ = p.run_host(B, want_v=True)
+        npix, n_half = p.npix, p.n_half
+        # the stage entries on the pipeline's arrays (after run_host: sky scaled, baselines made)
+        sky = vb.Sky()
+        sky.npix = npix
+        for k in ("B", "l", "m", "n", "cx", "cy", "cz", "cosA", "sinA"):
+            setattr(sky, k, p.ptr(k)[0])
+        sky.tile_pix = cfg.viss_tile_pix
+        bl = vb.Baselines()
+        bl.n_full, bl.nbl, bl.cosphi = 2 * n_half, p.nbl, p.cosphi
+        for k in ("u", "v", "w", "x1", "y1", "z1", "x2", "y2", "z2", "invn1", "invn2", "cosphi1", "cosphi2"):
+            setattr(bl, k, p.ptr(k)[0])
+        o1 = vb.Stage1Opts(precision=vb.PREC_FP32_FP64PH, cull=vb.CULL_TILECONE, phase_corrected=1, blockage=1)
+        need = vb.lib().vb_stage1_workspace_bytes(C.byref(sky), C.byref(bl), C.byref(o1))
+        ws = DeviceBuffer(need)
+        Va, Vb = zeros(2 * n_half, np.float64), zeros(2 * n_half, np.float64)
+        vb.check(vb.lib().vb_viss_halfsym(C.byref(sky), C.byref(bl), C.byref(o1), ws.ptr, need, Va.ptr, None, None))
+        vb.check(vb.lib().vb_stage1(C.byref(sky), C.byref(bl), C.byref(o1), ws.ptr, need, Vb.ptr, None))
+        vb.check(vb.lib().vb_synchronize())
+        assert np.array_equal(get(Va, np.float64).view(np.uint64), get(Vb, np.float64).view(np.uint64))
+        t0, tl = p.seg_plan()
+        o2 = vb.Stage2Opts(mirror=1, blockage=1, occ_mode=2, precision=vb.PREC_FP32_FP64PH, cull=vb.CULL_EXACT,
+                           grid_res=cfg.grid_res, bl_max=cfg.bl_max_m, lambda_=cfg.lambda_m)
+        need2 = vb.lib().vb_stage2_workspace_bytes(n_half, len(t0), npix, C.byref(o2))
+        ws2 = DeviceBuffer(need2)
+        Vh = dev(V1)
+        dt0, dtl = dev(np.asarray(t0, np.int32)), dev(np.asarray(tl, np.int32))
+        outs = []
+        for name in ("vb_recon_batched", "vb_stage2"):
+            Cb, Wb = zeros(npix), zeros(npix, np.uint32)
+            args = [C.byref(sky), C.byref(bl), Vh.ptr, len(t0), dt0.ptr, dtl.ptr, C.byref(o2), ws2.ptr, need2,
+                    Cb.ptr, Wb.ptr]
+            args += [None, None, None] if name == "vb_recon_batched" else [None]
+            vb.check(getattr(vb.lib(), name)(*args))
+            vb.check(vb.lib().vb_synchronize())
+            outs.append((get(Cb), get(Wb, np.uint32)))
+        assert np.array_equal(outs[0][0].view(np.uint32), outs[1][0].view(np.uint32))
+        assert np.array_equal(outs[0][1], outs[1][1])
+    C2 = np.empty(npix, np.float32)
+    V2 = np.empty(2 * n_half, np.float32)
+    rep = vb.Report()
+    vb.check(vb.lib().vb_run(C.byref(cfg), B.ctypes.data, 1, npix, C2.ctypes.data, V2.ctypes.data, C.byref(rep)))
+    assert np.array_equal(C1.view(np.uint32), C2.view(np.uint32))
+    assert np.array_equal(V1.view(np.uint32), V2.view(np.uint32))
+    assert rep.error_flags == 0
+    assert vb.lib().vb_run(C.byref(cfg), B.ctypes.data, 1, npix + 1, C2.ctypes.data, None, None) == 1   # VB_ERR_INVALID
+
+
 def test_graph_eager_determinism_and_host_entry(gpu, vb):
     kw = dict(nside=16, orbit_model=vb.ORBIT_SYNTHETIC, nsat=8, tsteps=48, segs=3, lambda_m=30.0, occ_R_m=6371e3,
               cull="exact", mirror=1, grid_res=101)

@@ -831,6 +831,7 @@ extern "C" int vb_pipeline_run_host(vb_pipeline* p, const float* B_host, int sca
   p->baselines_ready = true;
   vb_sky sky = sky_of(p);
   VB_TRY(stage1_prepare_pixels(&sky, p->p1, p->b1, p->s));
+  VB_CUDA(cudaMemsetAsync(p->b1.err, 0, sizeof(unsigned), p->s));   // as ensure_ready: a fresh error word
   p->pixels_ready = true;
   VB_TRY(run_once(p));
   VB_CUDA(cudaMemcpyAsync(C_host, p->C, p->npix * sizeof(float), cudaMemcpyDeviceToHost, p->s));
@@ -1050,6 +1051,20 @@ extern "C" int vb_pipeline_destroy(vb_pipeline* p) {
     pipeline_free(p);
   }
   return VB_OK;
+}
+
+extern "C" int vb_run(const vb_run_config* c, const float* B_host, int scale, int64_t npix_expected,
+                      float* C_host, float* V_half_host, vb_report* r) {
+  if (!c || !B_host || !C_host) return fail(VB_ERR_INVALID, "vb_run: null argument");
+  vb_pipeline* p = nullptr;
+  VB_TRY(vb_pipeline_create(c, &p));
+  int rc = VB_OK;
+  if (p->npix != npix_expected)
+    rc = fail(VB_ERR_INVALID, "vb_run: npix_expected=%lld, the configuration has %lld pixels",
+              (long long)npix_expected, (long long)p->npix);
+  if (rc == VB_OK) rc = vb_pipeline_run_host(p, B_host, scale, C_host, V_half_host, r);
+  vb_pipeline_destroy(p);
+  return rc;
 }
 
 // ---------------------------------------------------------------------------

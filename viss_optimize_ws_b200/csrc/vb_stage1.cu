@@ -787,3 +787,8 @@ extern "C" int vb_stage1_tile_classes(const vb_sky* sky, const vb_baselines* bl,
   VB_LAUNCH_CHECK();
   return VB_OK;
 }
+
+extern "C" int vb_stage1(const vb_sky* sky, const vb_baselines* bl, const vb_stage1_opts* o, void* workspace,
+                         size_t ws_bytes, double* V_half, void* stream) {
+  return vb_viss_halfsym(sky, bl, o, workspace, ws_bytes, V_half, nullptr, stream);
+}

@@ -1173,3 +1173,10 @@ extern "C" int vb_recon_batched(const vb_sky* sky, const vb_baselines* bl, const
   return stage2_run(sky, bl, V_half, nseg, seg_t0, seg_tlen, p, workspace, ws_bytes, C, W, seg_params, term_counters,
                     nullptr, as_stream(stream), nullptr);
 }
+
+extern "C" int vb_stage2(const vb_sky* sky, const vb_baselines* bl, const float* V_half, int nseg,
+                         const int* seg_t0, const int* seg_tlen, const vb_stage2_opts* o, void* workspace,
+                         size_t ws_bytes, float* C, uint32_t* W, void* stream) {
+  return vb_recon_batched(sky, bl, V_half, nseg, seg_t0, seg_tlen, o, workspace, ws_bytes, C, W, nullptr,
+                          nullptr, stream);
+}
