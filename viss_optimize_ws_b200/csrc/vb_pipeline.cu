@@ -534,6 +534,7 @@ static int enqueue_stages(vb_pipeline* p) {
   vb_sky sky = sky_of(p);
   vb_baselines bl = bl_of(p);
   VB_CUDA(cudaMemsetAsync(p->counters, 0, 8 * sizeof(unsigned long long), p->s));
+  VB_CUDA(cudaMemsetAsync(p->b1.err, 0, sizeof(unsigned), p->s));   // each run reports its own errors
   VB_CUDA(record_event(p->ev[0], p->s));
   VB_CUDA(cudaEventRecord(p->fork, p->s));
   VB_CUDA(cudaStreamWaitEvent(p->s_side, p->fork, 0));
@@ -831,7 +832,6 @@ extern "C" int vb_pipeline_run_host(vb_pipeline* p, const float* B_host, int sca
   p->baselines_ready = true;
   vb_sky sky = sky_of(p);
   VB_TRY(stage1_prepare_pixels(&sky, p->p1, p->b1, p->s));
-  VB_CUDA(cudaMemsetAsync(p->b1.err, 0, sizeof(unsigned), p->s));   // as ensure_ready: a fresh error word
   p->pixels_ready = true;
   VB_TRY(run_once(p));
   VB_CUDA(cudaMemcpyAsync(C_host, p->C, p->npix * sizeof(float), cudaMemcpyDeviceToHost, p->s));
