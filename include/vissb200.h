@@ -43,6 +43,23 @@ extern "C" {
 #define VB_ERR_HALFSYM      6   /* generated uvw violate the +/- pair layout */
 #define VB_ERR_IO           7   /* file could not be read or written */
 
+/* Bits of the device-side error word that the stage kernels set (atomicOr)
+ * while they run.  A flag does not stop the kernels: flagged terms are still
+ * summed (the access behind VB_DEVERR_BAD_INDEX excepted, which is skipped), so
+ * a non-zero word means the outputs of that call are not to be trusted.  The
+ * host reads the word after the stream has finished. */
+#define VB_DEVERR_WAIT_TIMEOUT  1u  /* a bounded device-side wait gave up */
+#define VB_DEVERR_BAD_INDEX     2u  /* an index check failed and the access was skipped */
+#define VB_DEVERR_HALFSYM       4u  /* the +/- pair layout of the baselines is violated */
+#define VB_DEVERR_PHASE_RANGE   8u  /* fp32_fp64phase: |u|+|v|+|w| of a term reached 2^28 turns, where
+                                       the exact range reduction no longer holds (stage 1: checked as
+                                       |u|, |v|, |w| >= 2^26 per baseline; stage 2: per group) */
+
+/* The device error word of the last vb_viss_halfsym / vb_stage1 /
+ * vb_recon_batched / vb_stage2 call that used this workspace (the word sits at
+ * its start).  Copies it on `stream` and synchronises that stream. */
+int vb_workspace_error_flags(const void* workspace, unsigned* flags, void* stream);
+
 /* Numeric precision of the direct sums (stage 1 and stage 2). */
 #define VB_PREC_REF32        0  /* FP32 phase, FP32 sincos, FP32 sums (upstream arithmetic) */
 #define VB_PREC_FP64         1  /* plain FP64 direct sum: FP64 phase, FP64 sincos, FP64 sums */
@@ -385,7 +402,8 @@ typedef struct {
   double   t_s1_kernel_ms; /* the stage-1 direct-sum kernel alone */
   double   t_s2_kernel_ms; /* the stage-2 reconstruction kernel alone */
   double   t_e2e_ms;       /* vb_pipeline_run_host: H2D, baselines, both stages, D2H */
-  int      error_flags;    /* device-side error word (0 = ok) */
+  int      error_flags;    /* OR of the stage-1 and stage-2 device error words of the run
+                              (VB_DEVERR_* bits, 0 = ok) */
   int      graph_kernels;  /* kernel nodes of the captured run graph (0 = eager) */
   double   bl_max_m;       /* bl_max the uv grids were built with (the automatic value when bl_max_m <= 0) */
 } vb_report;

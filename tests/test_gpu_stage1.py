@@ -365,3 +365,31 @@ def test_tilecone_subtile_refinement_is_bit_identical(case, vb, prec):
         V, c = stage1(sky, bl, precision=pm, cull=vb.CULL_TILECONE, refine_pix=r)
         assert np.array_equal(V.view(np.uint64), Voff.view(np.uint64)), r
         assert c[3] == coff[3] and c[1] <= coff[1] and c[0] >= coff[0] and c[2] >= coff[2]
+
+
+def test_device_error_word_in_the_workspace(vb, case):
+    """The stage-1 error word sits at the start of the caller's workspace and
+    is read with vb_workspace_error_flags: clear for in-range inputs, and the
+    fp32_fp64phase range bit when a baseline's |u| passes 2^26 wavelengths
+    (the exact range reduction needs |u|+|v|+|w| < 2^28 turns)."""
+    from gpu_util import DeviceBuffer
+    sky, bl = structs(case)
+    o = vb.Stage1Opts(precision=vb.PREC_FP32_FP64PH, cull=vb.CULL_TILECONE, phase_corrected=1, blockage=1)
+    need = vb.lib().vb_stage1_workspace_bytes(C.byref(sky), C.byref(bl), C.byref(o))
+    ws = DeviceBuffer(need)
+    V = zeros(case["n_full"], np.float64)
+    flags = C.c_uint(12345)
+    vb.check(vb.lib().vb_stage1(C.byref(sky), C.byref(bl), C.byref(o), ws.ptr, need, V.ptr, None))
+    vb.check(vb.lib().vb_workspace_error_flags(ws.ptr, C.byref(flags), None))
+    assert flags.value == 0
+    big = case["host"]["u"].copy()
+    big[5] = np.float32(1.0e8)                  # one baseline out of range (finite, no index involved)
+    du = dev(big)
+    bl.u = du.ptr
+    vb.check(vb.lib().vb_stage1(C.byref(sky), C.byref(bl), C.byref(o), ws.ptr, need, V.ptr, None))
+    vb.check(vb.lib().vb_workspace_error_flags(ws.ptr, C.byref(flags), None))
+    assert flags.value == 8                     # VB_DEVERR_PHASE_RANGE
+    bl.u = case["d"]["u"].ptr                    # the word is cleared by the next call
+    vb.check(vb.lib().vb_stage1(C.byref(sky), C.byref(bl), C.byref(o), ws.ptr, need, V.ptr, None))
+    vb.check(vb.lib().vb_workspace_error_flags(ws.ptr, C.byref(flags), None))
+    assert flags.value == 0

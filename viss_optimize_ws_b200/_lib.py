@@ -150,6 +150,7 @@ _SIGS = {
     "vb_stage2": (C.c_int, [C.POINTER(Sky), C.POINTER(Baselines), vp, C.c_int, vp, vp, C.POINTER(Stage2Opts),
                             vp, C.c_size_t, vp, vp, vp]),
     "vb_run": (C.c_int, [C.POINTER(RunConfig), vp, C.c_int, C.c_int64, vp, vp, C.POINTER(Report)]),
+    "vb_workspace_error_flags": (C.c_int, [vp, C.POINTER(C.c_uint), vp]),
     "vb_run_config_defaults": (None, [C.POINTER(RunConfig)]),
     "vb_pipeline_create": (C.c_int, [C.POINTER(RunConfig), C.POINTER(vp)]),
     "vb_pipeline_set_sky": (C.c_int, [vp, vp, C.c_int]),

@@ -40,6 +40,7 @@ enum : unsigned {
   ERR_WAIT_TIMEOUT = 1u << 0,   // a bounded wait gave up
   ERR_BAD_INDEX    = 1u << 1,   // an index check failed and the access was skipped
   ERR_HALFSYM      = 1u << 2,   // +/- pair layout violated
+  ERR_PHASE_RANGE  = 1u << 3,   // F32X phase outside its exact range (|u|+|v|+|w| >= 2^28 turns)
 };
 
 // Upstream half -> full signed index map (common.hpp:213-220 generalised to

@@ -652,9 +652,10 @@ static int fill_report(vb_pipeline* p, vb_report* r) {
   r->groups_total = g;
   r->stage1_terms = (long long)p->npix * p->n_half;
   r->stage2_terms = (long long)p->npix * g;
-  unsigned e1 = 0;
+  unsigned e1 = 0, e2 = 0;
   VB_CUDA(cudaMemcpy(&e1, p->b1.err, sizeof(unsigned), cudaMemcpyDeviceToHost));
-  r->error_flags = (int)e1;
+  if (p->ws2) VB_CUDA(cudaMemcpy(&e2, p->ws2, sizeof(unsigned), cudaMemcpyDeviceToHost));   // stage-2 word: offset 0
+  r->error_flags = (int)(e1 | e2);
   return VB_OK;
 }
 
@@ -1050,6 +1051,18 @@ extern "C" int vb_pipeline_destroy(vb_pipeline* p) {
     if (p->s) cudaStreamSynchronize(p->s);
     pipeline_free(p);
   }
+  return VB_OK;
+}
+
+static_assert(ERR_WAIT_TIMEOUT == VB_DEVERR_WAIT_TIMEOUT && ERR_BAD_INDEX == VB_DEVERR_BAD_INDEX &&
+                  ERR_HALFSYM == VB_DEVERR_HALFSYM && ERR_PHASE_RANGE == VB_DEVERR_PHASE_RANGE,
+              "device error bits of the header and the kernels differ");
+
+extern "C" int vb_workspace_error_flags(const void* workspace, unsigned* flags, void* stream) {
+  if (!workspace || !flags) return fail(VB_ERR_INVALID, "vb_workspace_error_flags: null argument");
+  cudaStream_t s = as_stream(stream);
+  VB_CUDA(cudaMemcpyAsync(flags, workspace, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+  VB_CUDA(cudaStreamSynchronize(s));
   return VB_OK;
 }
 

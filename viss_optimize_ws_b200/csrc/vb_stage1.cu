@@ -251,7 +251,7 @@ __global__ void __maxnreg__(MINB == 3 ? 80 : 120) k_stage1(const S1Args a) {
       if (MODE == VB_PREC_FP32_FP64PH && b.active &&
           (fabsf(uu) >= (float)kMaxUvwF32X || fabsf(vv) >= (float)kMaxUvwF32X ||
            fabsf(ww) >= (float)kMaxUvwF32X))
-        atomicOr(a.err, ERR_BAD_INDEX);
+        atomicOr(a.err, ERR_PHASE_RANGE);
     }
 
     double accR[BPT], accI[BPT];
@@ -633,6 +633,7 @@ int stage1_plan(const vb_sky* sky, const vb_baselines* bl, const vb_stage1_opts*
 size_t stage1_carve(const Stage1Plan& p, void* ws, size_t cap, Stage1Buffers* b, bool pack_pixels) {
   Carve c(ws, cap);
   Stage1Buffers x;
+  x.err = c.take<unsigned>(4);   // first: vb_workspace_error_flags reads it at offset 0
   if (pack_pixels) {
     x.lm = c.take<double2>(p.npix);
     x.nb = c.take<float4>(p.npix);
@@ -642,7 +643,6 @@ size_t stage1_carve(const Stage1Plan& p, void* ws, size_t cap, Stage1Buffers* b,
   }
   x.partial = c.take<double2>((size_t)p.nchunk * (size_t)p.n_half);
   x.queue = c.take<int>(4);
-  x.err = c.take<unsigned>(4);
   if (b) *b = x;
   if (ws && !c.ok) return 0;
   return c.used();

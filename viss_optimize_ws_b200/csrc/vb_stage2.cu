@@ -260,7 +260,7 @@ __global__ void k_group_records(const RecArgs r, int max_groups) {
     o.fa = q.fa;
     o.fb = q.fb;
     // the F32X phase needs |a l + b m + c n| < 2^28 turns (kMagic2)
-    if (fabs(o.a) + fabs(o.b) + fabs(o.c) >= 268435456.0) atomicOr(r.err, ERR_BAD_INDEX);
+    if (fabs(o.a) + fabs(o.b) + fabs(o.c) >= 268435456.0) atomicOr(r.err, ERR_PHASE_RANGE);
     o.vx = o.vy = 0.f;
     o.cp1 = o.cp2 = r.cosphi;
     o.p1 = o.p2 = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -863,6 +863,7 @@ struct S2Slices {
 static size_t carve2(const Stage2Plan& p, void* ws, size_t cap, S2Slices* s) {
   Carve c(ws, cap);
   S2Slices x{};
+  x.err = c.take<unsigned>(4);   // first: vb_workspace_error_flags reads it at offset 0
   const size_t n = (size_t)(p.n_keyed_total > 0 ? p.n_keyed_total : 1);
   x.sp = c.take<vb_seg_params>(p.nseg);
   x.k0 = c.take<unsigned long long>(n);
@@ -874,7 +875,6 @@ static size_t carve2(const Stage2Plan& p, void* ws, size_t cap, S2Slices* s) {
   x.start = c.take<int>(n + 1);
   x.ngroups = c.take<int>(4);
   x.queue = c.take<int>(4);
-  x.err = c.take<unsigned>(4);
   x.wsum = c.take<double>(2);
   x.rec = c.take<GroupRec>(n);
   x.meta = c.take<GroupMeta>(n);
