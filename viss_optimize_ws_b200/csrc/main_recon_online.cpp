@@ -401,6 +401,10 @@ int main(int argc, char** argv) {
     } else if (vb_pipeline_run(p, &rep) != VB_OK) {
       return die(std::string("ERROR ") + vb_last_error());
     }
+    if (rep.error_flags != 0)   // stderr only: stdout keeps the upstream lines
+      std::cerr << "WARNING day " << dayid << ": device error flags " << rep.error_flags
+                << ((rep.error_flags & VB_DEVERR_PHASE_RANGE) ? " (uvw beyond the fp32_fp64phase range; use --precision=fp64)" : "")
+                << ": this day's outputs are not to be trusted" << std::endl;
     std::vector<vb_seg_params> sp(nseg);
     vb_pipeline_seg_params(p, sp.data());
     Dev dv{p};
