@@ -37,6 +37,12 @@ namespace vb {
 
 constexpr int S1_THREADS = 256;
 constexpr int kClsHid = 0, kClsVis = 1, kClsMix = 2;
+// Kernel-internal cull variant: tile-cone culling whose visible tiles still take
+// the per-pixel test (vb_stage1_opts.mask_visible_tiles).  A template value of
+// its own, so that the default tile-cone kernel carries no extra test.
+constexpr int kCullTileconeMV = 3;
+template <int CULL>
+__host__ __device__ constexpr bool is_tilecone() { return CULL == VB_CULL_TILECONE || CULL == kCullTileconeMV; }
 
 // F32X phase reduction: magic = 1.5 * 2^29 keeps every partial sum of the FMA
 // chain in [2^29, 2^30) (|u| + |v| + |w| < 2^28); the double's ulp is then
@@ -111,13 +117,13 @@ template <int CULL>
 __device__ __forceinline__ int tile_class(const S1Args& a, const Baseline& b, int tile_id) {
   if (!b.active) return kClsHid;
   if (!a.blockage) return kClsVis;
-  if constexpr (CULL == VB_CULL_TILECONE) {
+  if constexpr (is_tilecone<CULL>()) {
     const float cx = a.tcx[tile_id], cy = a.tcy[tile_id], cz = a.tcz[tile_id];
     const float cA = a.tcosA[tile_id], sA = a.tsinA[tile_id];
     bool vis1, hid1, vis2, hid2;
     cone_classify(cone_dot(b.ux1, b.uy1, b.uz1, cx, cy, cz), cA, sA, b.c1, vis1, hid1);
     cone_classify(cone_dot(b.ux2, b.uy2, b.uz2, cx, cy, cz), cA, sA, b.c2, vis2, hid2);
-    return (hid1 || hid2) ? kClsHid : ((vis1 && vis2 && !a.mask_visible) ? kClsVis : kClsMix);
+    return (hid1 || hid2) ? kClsHid : ((vis1 && vis2 && CULL != kCullTileconeMV) ? kClsVis : kClsMix);
   } else if constexpr (CULL == VB_CULL_EXACT) {
     return exact_tile_class(a.cones + tile_id, b.x1, b.y1, b.z1, b.i1, b.c1, b.x2, b.y2, b.z2, b.i2, b.c2);
   } else {
@@ -126,7 +132,8 @@ __device__ __forceinline__ int tile_class(const S1Args& a, const Baseline& b, in
 }
 
 __device__ __forceinline__ int tile_class_rt(const S1Args& a, const Baseline& b, int tile_id) {
-  if (a.cull == VB_CULL_TILECONE) return tile_class<VB_CULL_TILECONE>(a, b, tile_id);
+  if (a.cull == VB_CULL_TILECONE)
+    return a.mask_visible ? tile_class<kCullTileconeMV>(a, b, tile_id) : tile_class<VB_CULL_TILECONE>(a, b, tile_id);
   if (a.cull == VB_CULL_EXACT) return tile_class<VB_CULL_EXACT>(a, b, tile_id);
   return tile_class<VB_CULL_NONE>(a, b, tile_id);
 }
@@ -286,7 +293,7 @@ __global__ void __maxnreg__(MINB == 3 ? 80 : 120) k_stage1(const S1Args a) {
       const bool warp_live = __any_sync(0xffffffffu, any_live);
       const bool warp_mix = __any_sync(0xffffffffu, any_mix);
       // mixed tiles refined into exact sub-tiles count their terms per sub-tile
-      const bool refine = (CULL == VB_CULL_TILECONE) && warp_mix && a.refine_pix > 0;
+      const bool refine = is_tilecone<CULL>() && warp_mix && a.refine_pix > 0;
       const int64_t tile_terms = (int64_t)nact * (t1 - t0);
       cnt_all += tile_terms;
       if (!warp_live) cnt_hid += tile_terms;
@@ -524,6 +531,7 @@ static void* stage1_kernel(int bpt, int minb) {
 template <int MODE>
 static void* stage1_kernel_cull(int bpt, int minb, int cull) {
   if (cull == VB_CULL_TILECONE) return stage1_kernel<MODE, VB_CULL_TILECONE>(bpt, minb);
+  if (cull == kCullTileconeMV) return stage1_kernel<MODE, kCullTileconeMV>(bpt, minb);
   if (cull == VB_CULL_EXACT) return stage1_kernel<MODE, VB_CULL_EXACT>(bpt, minb);
   return stage1_kernel<MODE, VB_CULL_NONE>(bpt, minb);
 }
@@ -603,7 +611,7 @@ int stage1_plan(const vb_sky* sky, const vb_baselines* bl, const vb_stage1_opts*
   const int per_tile = S1_THREADS * q.bpt;
   q.n_btile = (int)ceil_div(q.n_half, per_tile);
   size_t smem = (size_t)stage * 48;
-  int occ = occupancy(q.precision, q.bpt, q.minb, q.cull, smem);
+  int occ = occupancy(q.precision, q.bpt, q.minb, q.mask_visible ? kCullTileconeMV : q.cull, smem);
   int capacity = sm_count() * occ;
   q.grid = capacity;
   // enough items per CTA that the dynamic queue's tail (one item) stays short
@@ -678,7 +686,7 @@ int stage1_run(const vb_sky* sky, const vb_baselines* bl, const Stage1Plan& p, c
   a.queue = b.queue; a.partial = b.partial; a.counters = counters; a.err = b.err;
   VB_CUDA(cudaMemsetAsync(b.queue, 0, sizeof(int), s));
   size_t smem = (size_t)p.stage_pix * 48;
-  const void* kern = stage1_kernel_of(p.precision, p.bpt, p.minb, p.cull);
+  const void* kern = stage1_kernel_of(p.precision, p.bpt, p.minb, p.mask_visible ? kCullTileconeMV : p.cull);
   VB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   void* args[] = {&a};
   if (kbeg) VB_CUDA(record_event(kbeg, s));
