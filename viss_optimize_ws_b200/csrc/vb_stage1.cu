@@ -375,6 +375,9 @@ __global__ void __maxnreg__(MINB == 3 ? 80 : 120) k_stage1(const S1Args a) {
         // pixels [j0, j1) of the staged tile (j0 even: pixel parity = index parity)
         auto run = [&](const int j0, const int j1, auto path_tag) {
           int j = j0;
+          // two pixel pairs per trip: 0.5 % faster than the compiler's choice
+          // (no unroll 1: +5 %, unroll 3 / 4: +5-6 %)
+#pragma unroll 2
           for (; j + 1 < j1; j += 2) {
             pixel(j, pR0, pI0, path_tag, Even{});
             pixel(j + 1, pR1, pI1, path_tag, Odd{});
