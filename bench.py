@@ -55,6 +55,12 @@ def workload_kwargs(prec: str = "fp32_fp64phase") -> dict:
                 grid_res=513, bl_max_m=0.0, orbit_seed=42, precision=prec, occ_mode=2, blockage=1)
 
 
+def rank_workload_kwargs(local: int, prec: str = "fp32_fp64phase") -> dict:
+    """workload_kwargs on this rank's GPU: the pipeline selects `device` itself
+    on every call, so each rank must name its own (torchrun's LOCAL_RANK)."""
+    return dict(workload_kwargs(prec), device=local)
+
+
 # The five workloads of the metric's definition (synthetic stand-ins with the
 # stated shapes; seeds recorded).  The second is the headline line of main();
 # `--config N` prints a report line for any of them.
@@ -534,7 +540,7 @@ def run_sharded_bench(args) -> None:
     dist = Dist(ws, local)
     vb.check(vb.lib().vb_set_device(local))
     B = vb.synthetic_sky(256, seed=1)
-    p = vb.Pipeline(vb.run_config(**workload_kwargs()))
+    p = vb.Pipeline(vb.run_config(**rank_workload_kwargs(local)))
     p.set_sky(B)
     p.make_baselines()
     comp = sharded.GpuCompute(vb, p)
@@ -597,7 +603,7 @@ def main() -> None:
     vb.check(L.vb_measure_peaks(C.byref(sfu), C.byref(f32), C.byref(f64), C.byref(clk)))
 
     B = vb.synthetic_sky(256, seed=1)
-    kw = workload_kwargs()
+    kw = rank_workload_kwargs(local)
     if args.shape not in ("auto", "default"):
         s1, s2 = args.shape.split("/")
         b, sp, ct, it = (int(x) for x in s1.split(","))
@@ -671,7 +677,7 @@ def main() -> None:
     # plain FP64 GPU build of the same pipeline: speed and errors
     fp64 = None
     if not args.no_fp64:
-        q = vb.Pipeline(vb.run_config(**workload_kwargs("fp64")))
+        q = vb.Pipeline(vb.run_config(**rank_workload_kwargs(local, "fp64")))
         q.set_sky(B)
         q.make_baselines()
         tune64 = q.autotune(reps=1) if args.shape == "auto" else None   # the FP64 build gets its own best shapes

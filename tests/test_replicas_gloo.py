@@ -65,3 +65,18 @@ def test_rank_failure_is_reported_not_hung():
     states = {o[0]: o[1] for o in out}
     assert states[1] == "error"
     assert states[0] == "error"       # the surviving rank's barrier ends with an error
+
+
+def test_each_rank_builds_its_pipeline_on_its_own_gpu(vb):
+    """Under torchrun every rank's pipeline must name its LOCAL_RANK device: the
+    library selects the configured device on every call, so a config left at
+    the default would put every rank on GPU 0."""
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    import bench
+    for local in (0, 3, 7):
+        kw = bench.rank_workload_kwargs(local)
+        assert kw["device"] == local
+        assert vb.run_config(**kw).device == local
+        assert {k: v for k, v in kw.items() if k != "device"} == bench.workload_kwargs()
+    assert bench.rank_workload_kwargs(5, "fp64")["precision"] == "fp64"
