@@ -80,3 +80,38 @@ def test_struct_layouts_match_bindings(vb):
     text = (ROOT / "include" / "vissb200.h").read_text()
     declared = set(re.findall(r"}\s*(vb_[a-z0-9_]+)\s*;", text))
     assert declared == set(ABI_STRUCTS), declared ^ set(ABI_STRUCTS)
+
+
+def test_plain_c_caller_compiles_links_and_runs(tmp_path, vb):
+    """The header is plain C (a cgo / FFI binding includes it as such): a C99
+    program that includes it, links libvissb200 and calls the host-only entry
+    points builds with -Wall -Werror and runs without a GPU."""
+    from viss_optimize_ws_b200._lib import LIB_PATH
+    src = tmp_path / "caller.c"
+    src.write_text(r'''
+#include <stdio.h>
+#include <string.h>
+#include "vissb200.h"
+int main(void) {
+  vb_run_config c;
+  vb_run_config_defaults(&c);
+  if (c.nm1_fast != 1 || c.use_graph != 1) return 2;
+  if (vb_abi_sizeof("vb_run_config") != sizeof(vb_run_config)) return 3;
+  if (vb_abi_sizeof("vb_stage1_opts") != sizeof(vb_stage1_opts)) return 4;
+  if (vb_abi_sizeof("vb_report") != sizeof(vb_report)) return 5;
+  int R = 0, half = 0; float du = 0.f;
+  if (vb_grid_params(0.f, 0.f, 100e3f, 30.f, 0, &R, &half, &du) != VB_OK) return 6;
+  if (vb_run(NULL, NULL, 1, 0, NULL, NULL, NULL) != VB_ERR_INVALID) return 7;
+  printf("%d %d %s\n", R, half, vb_error_string(VB_ERR_INVALID));
+  return 0;
+}
+''')
+    exe = tmp_path / "caller"
+    r = subprocess.run(["gcc", "-std=c99", "-Wall", "-Wextra", "-Werror", "-I", str(ROOT / "include"), str(src),
+                        "-o", str(exe), "-L", str(LIB_PATH.parent), "-lvissb200",
+                        f"-Wl,-rpath,{LIB_PATH.parent}"], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    run = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120)
+    assert run.returncode == 0, (run.returncode, run.stderr)
+    R, half, msg = run.stdout.split(maxsplit=2)
+    assert int(R) % 2 == 1 and int(half) == (int(R) - 1) // 2 and msg.strip()
