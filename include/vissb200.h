@@ -238,16 +238,25 @@ int vb_viss_halfsym(const vb_sky* sky, const vb_baselines* bl,
  * The caller passes only inputs and outputs.  No counterpart in the upstream
  * project (upstream allocates everything in main()).
  * Scratch is one file-scope device array of VB_VISS_NOALLOC_MAX_BYTES that
- * every GPU which loads the library holds until the process exits; a sky /
- * baseline set that needs more (about npix * 48 bytes + partial sums, e.g.
- * nside >= 512) returns VB_ERR_UNSUPPORTED.  The first call on a device looks
- * up the array's device address, so make that first call before any stream
- * capture.  All calls share the one array and it keeps the last call's
- * contents: calls that overlap on the GPU (other streams or threads) race.
- * No cudaMalloc, cudaFree or allocating library routine is called. */
+ * every GPU which loads the library holds until the process exits.  Under
+ * CUDA's default lazy module loading the array is reserved at the first call
+ * on each device, and that call can fail with out-of-memory: hosts with their
+ * own allocator should make the first call before that allocator takes its
+ * budget (or run with CUDA_MODULE_LOADING=EAGER), and before any stream
+ * capture.  Every call looks up the array's address in the current context.
+ * A sky / baseline set that needs more scratch (about npix * 48 bytes +
+ * partial sums, e.g. nside >= 512) returns VB_ERR_UNSUPPORTED.  With
+ * o->chunk_pix = 0 the pixel chunks may be widened until the partial sums fit;
+ * a chunk_pix the caller sets is kept, and a plan that does not fit with it
+ * returns VB_ERR_UNSUPPORTED.  All calls share the one array and it keeps the
+ * last call's contents: calls that overlap on the GPU (other streams or
+ * threads) race.  error_flags (nullable, device, one uint32) receives this
+ * call's VB_DEVERR_* bits on `stream`.  No cudaMalloc, cudaFree or allocating
+ * library routine is called. */
 int vb_viss_halfsym_noalloc(const vb_sky* sky, const vb_baselines* bl,
                             const vb_stage1_opts* o, double* V_half,
-                            unsigned long long* term_counters, void* stream);
+                            unsigned long long* term_counters,
+                            unsigned* error_flags, void* stream);
 
 /* Phase correction V *= exp(-2 pi i w) (skipped when already_corrected) in
  * FP64, then float32 outputs: V_half_out (2*n_half floats) and, if non-NULL,

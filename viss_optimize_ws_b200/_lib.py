@@ -133,7 +133,7 @@ _SIGS = {
     "vb_viss_halfsym": (C.c_int, [C.POINTER(Sky), C.POINTER(Baselines), C.POINTER(Stage1Opts), vp, C.c_size_t,
                                   vp, vp, vp]),
     "vb_viss_halfsym_noalloc": (C.c_int, [C.POINTER(Sky), C.POINTER(Baselines), C.POINTER(Stage1Opts), vp, vp,
-                                          vp]),
+                                          vp, vp]),
     "vb_stage1_tile_classes": (C.c_int, [C.POINTER(Sky), C.POINTER(Baselines), C.POINTER(Stage1Opts), vp,
                                          C.c_size_t, vp, C.POINTER(C.c_int), vp]),
     "vb_phase_correct_expand": (C.c_int, [vp, vp, C.c_int, C.c_int, C.c_int, vp, vp, vp]),
