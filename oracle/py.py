@@ -62,6 +62,9 @@ def oracle() -> C.CDLL:
                                                                                                 C.c_int,
                                                                                                 C.c_int, vp,
                                                                                                 vp]),
+            "or_stage1_subset_simd": (None, [i64, vp, vp, vp, vp, C.c_int] + [vp] * 13 + [f32, C.c_int, vp, vp]),
+            "or_stage2_subset_simd": (C.c_int, [i64, vp, vp, vp, C.c_int, C.c_int, vp, vp] + [vp] * 13
+                                      + [f32, vp, f32, f32, C.c_int, C.c_int, vp, vp, vp, vp]),
             "or_reference_plan": (None, [f32, vp, vp, vp]),
             "or_window_starts": (None, [f32, C.c_int, C.c_uint64, vp]),
             "or_make_sky": (None, [C.c_int, C.c_uint64, C.c_int, f32, vp]),

@@ -110,6 +110,23 @@ void or_syn_baselines(int nsat, int T, double dt_s, double alt_min, double alt_m
                       double R_km, uint64_t seed, int day, float lambda_m, float* u, float* v, float* w, float* x1,
                       float* y1, float* z1, float* x2, float* y2, float* z2, float* in1, float* in2);
 
+/* Vectorised CPU baseline of the upstream FP32 arithmetic (vb_oracle_simd.cpp):
+ * the timed CPU leg of bench.py only, not a checker.  Stage 1 over the listed
+ * half-baselines (V: 2 doubles each); stage 2 (mirror, occ_mode 2) over the
+ * listed pixels, returning the number of gridded groups (t_group_s: the
+ * grouping's time). */
+void or_stage1_subset_simd(int64_t npix, const float* B, const float* l, const float* m, const float* n, int nbl,
+                           const float* u, const float* v, const float* w, const float* x1, const float* y1,
+                           const float* z1, const float* in1, const float* x2, const float* y2, const float* z2,
+                           const float* in2, const float* cp1, const float* cp2, float cosphi, int nsub,
+                           const int* ih_list, double* V);
+int or_stage2_subset_simd(int64_t npix, const float* l, const float* m, const float* n, int nbl, int nseg,
+                          const int* seg_t0, const int* seg_tlen, const float* u, const float* v, const float* w,
+                          const float* x1, const float* y1, const float* z1, const float* in1, const float* x2,
+                          const float* y2, const float* z2, const float* in2, const float* cp1, const float* cp2,
+                          float cosphi, const float* V_half, float bl_max, float lambda, int grid_res, int npx,
+                          const int64_t* pix, double* Cout, uint32_t* Wout, double* t_group_s);
+
 #ifdef __cplusplus
 }
 #endif

@@ -78,5 +78,5 @@ def test_each_rank_builds_its_pipeline_on_its_own_gpu(vb):
         kw = bench.rank_workload_kwargs(local)
         assert kw["device"] == local
         assert vb.run_config(**kw).device == local
-        assert {k: v for k, v in kw.items() if k != "device"} == bench.workload_kwargs()
+        assert {k: v for k, v in kw.items() if k != "device"} == bench.config_kwargs(bench.HEADLINE)
     assert bench.rank_workload_kwargs(5, "fp64")["precision"] == "fp64"
