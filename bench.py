@@ -583,41 +583,43 @@ def run_config_report(args) -> None:
 
 def run_sharded_bench(args) -> None:
     """--mode sharded: one day of the headline workload split over the ranks
-    (viss_optimize_ws_b200/sharded.py; NCCL all-gather of V and gather of C),
-    timed per rank with CUDA events around the whole day (exchange included),
-    max over ranks; strong scaling."""
+    (viss_optimize_ws_b200/sharded.py, run_day_device: NCCL all-gather of V
+    into device memory, gather of C / W to rank 0's device memory), timed per
+    rank with CUDA events around the whole day (exchange included), max over
+    ranks; strong scaling."""
     import torch
     import viss_optimize_ws_b200 as vb
     from viss_optimize_ws_b200 import sharded
     ws, rank, local = dist_env()
     dist = Dist(ws, local)
     vb.check(vb.lib().vb_set_device(local))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
     kw = rank_workload_kwargs(local)
     B = vb.synthetic_sky(kw["nside"], seed=1)
     p = vb.Pipeline(vb.run_config(**kw))
     p.set_sky(B)
     p.make_baselines()
     comp = sharded.GpuCompute(vb, p)
-    dev = torch.device("cuda", local) if ws > 1 else torch.device("cpu")
     if ws > 1:
-        ex = sharded.TorchExchange(dist.td, dev)
+        ex = sharded.DeviceExchange(dist.td, dev)
     else:
         class _Local:
-            def all_gather(self, piece, sizes, r):
-                return piece
+            def all_gather_into(self, out, piece, sizes):
+                out[: piece.numel()].copy_(piece)
 
-            def gather0(self, piece, sizes, r):
-                return piece
+            def gather0_into(self, out, piece, sizes, r):
+                out[: piece.numel()].copy_(piece)
         ex = _Local()
     steps = p.n_half // p.nbl
     for _ in range(args.warmup):
-        sharded.run_day(comp, ex, rank if ws > 1 else 0, ws, steps, p.nbl, p.npix)
+        sharded.run_day_device(comp, ex, rank, ws, steps, p.nbl, p.npix, dev)
     dist.barrier()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
     for _ in range(args.steps):
-        sharded.run_day(comp, ex, rank if ws > 1 else 0, ws, steps, p.nbl, p.npix)
+        sharded.run_day_device(comp, ex, rank, ws, steps, p.nbl, p.npix, dev)
     e1.record()
     torch.cuda.synchronize()
     dist.barrier()
@@ -628,10 +630,10 @@ def run_sharded_bench(args) -> None:
         print(json.dumps({"metric": METRIC, "value": terms * args.steps / (t * 1e-3) / 1e9, "unit": UNIT,
                           "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t / args.steps,
                           "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
-                          "dtype": "f32+f64phase", "data": "synthetic",
-                          "config": dict(WORKLOAD, parallelism=f"sharded{ws}",
-                                         note="stage 1 by time steps + all-gather of V, stage 2 by pixels + "
-                                              "gather of C; host-orchestrated exchange")}), flush=True)
+                          "dtype": "f32+f64phase", "data": "synthetic", "config": WORKLOAD,
+                          "run": {"parallelism": f"sharded{ws}",
+                                  "note": "stage 1 by time steps + NCCL all-gather of V into device memory, stage 2 "
+                                          "by pixels + gather of C / W to rank 0's device memory"}}), flush=True)
     p.close()
     dist.close()
 

@@ -2,8 +2,9 @@
 with the real kernels: two ranks as two processes that share this GPU and
 exchange V and C over gloo on the host (their kernels never wait on each
 other); the sharded day equals the single-GPU day to FP32 summation
-rounding, with identical visible-group counts.  A second test runs the day as
-one rank over NCCL with device tensors, the exchange a multi-GPU run uses."""
+rounding, with identical visible-group counts.  A second test runs the
+device-resident day as one rank over NCCL (V and C never leave device
+memory), the exchange a multi-GPU run uses."""
 from __future__ import annotations
 
 import os
@@ -51,9 +52,29 @@ def _worker(rank, ws, port, q):
         q.put((rank, "error", repr(e)[:300], None, None))
 
 
+class NoHostCopy:
+    """The library handle with every host<->device copy refused: what the
+    device-resident day must never do."""
+
+    def __init__(self, L):
+        self._L = L
+
+    def __getattr__(self, name):
+        f = getattr(self._L, name)
+        if name == "vb_memcpy":
+            def guarded(dst, src, n, kind):
+                if kind != 2:
+                    raise AssertionError(f"host copy of {n} bytes during the device-resident day")
+                return f(dst, src, n, kind)
+            return guarded
+        return f
+
+
 def _worker_nccl(port, q):
-    """One rank over NCCL with device tensors: the exchange path a multi-GPU
-    run takes, on the one GPU this test has (a one-rank all-gather is a copy)."""
+    """One rank over NCCL, every piece in device memory (run_day_device): the
+    exchange path a multi-GPU run takes, on the one GPU this test has (a
+    one-rank collective is a device copy).  Host copies of V or C are refused
+    while the day runs."""
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), NCCL_NVLS_ENABLE="0")
     import sys
     sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
@@ -65,14 +86,24 @@ def _worker_nccl(port, q):
     from viss_optimize_ws_b200 import sharded
     try:
         torch.cuda.set_device(0)
+        dev = torch.device("cuda", 0)
         td.init_process_group("nccl", rank=0, world_size=1, timeout=datetime.timedelta(seconds=120),
-                              device_id=torch.device("cuda", 0))
+                              device_id=dev)
         with vb.Pipeline(vb.run_config(**KW)) as p:
             p.set_sky(vb.synthetic_sky(32, seed=8))
             p.make_baselines()
             comp = sharded.GpuCompute(vb, p)
-            ex = sharded.TorchExchange(td, torch.device("cuda", 0))
-            V, Cc, W = sharded.run_day(comp, ex, 0, 1, p.n_half // p.nbl, p.nbl, p.npix)
+            ex = sharded.DeviceExchange(td, dev)
+            comp.L = NoHostCopy(comp.L)
+            to_array = vb.DeviceBuffer.to_array
+            vb.DeviceBuffer.to_array = lambda *a, **k: (_ for _ in ()).throw(AssertionError("download"))
+            try:
+                for _ in range(2):
+                    Vt, Ct, Wt = sharded.run_day_device(comp, ex, 0, 1, p.n_half // p.nbl, p.nbl, p.npix, dev)
+                torch.cuda.synchronize()
+            finally:
+                vb.DeviceBuffer.to_array = to_array
+            V, Cc, W = Vt.cpu().numpy(), Ct.cpu().numpy(), Wt.cpu().numpy().view(np.uint32)
         td.destroy_process_group()
         q.put(("ok", V, Cc, W))
     except Exception as e:

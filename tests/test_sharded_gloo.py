@@ -121,3 +121,84 @@ def test_sharded_day_equals_single_process():
         else:
             assert Cc is None and W is None
     assert (W1 > 0).any()
+
+
+class OracleDeviceCompute(OracleCompute):
+    """CPU stand-in for GpuCompute's device-resident methods: the same pieces
+    as CPU torch tensors, so that run_day_device and DeviceExchange run their
+    collective steps over gloo."""
+
+    def full_buffers(self, device):
+        import torch
+        self._full = {"V": torch.zeros(2 * self.nbl * T, dtype=torch.float32),
+                      "C": torch.zeros(self.npix, dtype=torch.float32),
+                      "W": torch.zeros(self.npix, dtype=torch.int32)}
+        return dict(self._full, V_ptr=None)
+
+    def stage1_device(self, lo, hi, device):
+        import torch
+        return torch.from_numpy(self.stage1(lo, hi).copy())
+
+    def stage2_device(self, V_ptr, plo, phi, device):
+        import torch
+        Cc, W = self.stage2(self._full["V"].numpy(), plo, phi)
+        return torch.from_numpy(Cc.copy()), torch.from_numpy(W.astype(np.int32))
+
+
+def _worker_device(rank, ws, port, q):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+    import datetime
+
+    import torch
+    import torch.distributed as td
+    try:
+        td.init_process_group("gloo", rank=rank, world_size=ws, timeout=datetime.timedelta(seconds=60))
+        ex = sharded.DeviceExchange(td, torch.device("cpu"))
+        # unequal pieces: rank r contributes r + 2 values r*100 + i
+        sizes = [r + 2 for r in range(ws)]
+        piece = torch.tensor([rank * 100 + i for i in range(sizes[rank])], dtype=torch.float32)
+        out = torch.full((sum(sizes),), -1.0)
+        ex.all_gather_into(out, piece, sizes)
+        g = torch.full((sum(sizes),), -1.0) if rank == 0 else None
+        ex.gather0_into(g, piece, sizes, rank)
+        comp = OracleDeviceCompute()
+        V, Cc, W = sharded.run_day_device(comp, ex, rank, ws, T, comp.nbl, comp.npix, torch.device("cpu"))
+        q.put((rank, "ok", out.numpy(), None if g is None else g.numpy(), V.numpy().copy(),
+               Cc.numpy().copy() if rank == 0 else None, W.numpy().copy() if rank == 0 else None))
+        td.destroy_process_group()
+    except Exception as e:
+        q.put((rank, "error", repr(e)[:300], None, None, None, None))
+
+
+def test_device_exchange_and_day_over_two_ranks():
+    """DeviceExchange (padded all-gather into a destination, gather to rank 0
+    only) with unequal pieces, and run_day_device with the oracle standing in
+    for the kernels: world size 2 over gloo equals the single-process day bit
+    for bit; C and W are complete on rank 0."""
+    comp = OracleCompute()
+    V1, C1, W1 = sharded.run_day(comp, LocalExchange(), 0, 1, T, comp.nbl, comp.npix)
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = free_port()
+    procs = [ctx.Process(target=_worker_device, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    out = sorted([q.get(timeout=180) for _ in range(2)], key=lambda o: o[0])
+    for p in procs:
+        p.join(timeout=60)
+        if p.is_alive():
+            p.kill()
+    assert [o[1] for o in out] == ["ok", "ok"], out
+    expect = np.array([0, 1, 100, 101, 102], np.float32)
+    for rank, _, ag, g, V, Cc, W in out:
+        assert np.array_equal(ag, expect)
+        assert np.array_equal(V.view(np.uint32), V1.view(np.uint32))
+        if rank == 0:
+            assert np.array_equal(g, expect)
+            assert np.array_equal(Cc.view(np.uint32), C1.view(np.uint32))
+            assert np.array_equal(W.astype(np.uint32), W1)
+        else:
+            assert g is None
