@@ -118,6 +118,9 @@ def parse() -> argparse.Namespace:
                          "(strong scaling: stage 1 by time steps + all-gather of V, stage 2 by pixels + gather of C)")
     ap.add_argument("--config", type=int, default=0,
                     help="print a report line for configuration 1-5 instead of the headline line")
+    ap.add_argument("--day-fraction", type=int, default=1,
+                    help="run 1/F of the headline day (time steps and segments divided by F): a smaller case of "
+                         "the same kernels for profiler captures; the line then names the reduced workload")
     ap.add_argument("--shape", default="auto",
                     help="kernel shapes: 'auto' (autotuned before the warm-up, untimed), 'default' (built-in), "
                          "or 'bpt,stage_pix,ctas_per_sm,items_per_cta/ppt,items_per_cta' for stage 1 / stage 2")
@@ -724,6 +727,11 @@ def main() -> None:
     vb.check(L.vb_measure_peaks(C.byref(sfu), C.byref(f32), C.byref(f64), C.byref(clk)))
 
     kw = rank_workload_kwargs(local)
+    workload = WORKLOAD
+    if args.day_fraction > 1:
+        f = args.day_fraction
+        kw = dict(kw, tsteps=max(1, kw["tsteps"] // f), segs=max(1, kw["segs"] // f))
+        workload = dict(WORKLOAD, workload=f"{WORKLOAD['workload']}_day1of{f}", tsteps=kw["tsteps"], segs=kw["segs"])
     B = vb.synthetic_sky(kw["nside"], seed=1)
     p, shape_info = tuned_pipeline(vb, kw, B, 16, args.shape)
     shape = shape_string(p.cfg)
@@ -788,7 +796,8 @@ def main() -> None:
     # plain FP64 GPU build of the same pipeline: speed and errors
     fp64 = None
     if not args.no_fp64:
-        q, info64 = tuned_pipeline(vb, rank_workload_kwargs(local, "fp64"), B, 64, args.shape)
+        kw64 = dict(kw, precision="fp64")
+        q, info64 = tuned_pipeline(vb, kw64, B, 64, args.shape)
         q.run()
         tq = []
         for _ in range(2):
@@ -821,7 +830,7 @@ def main() -> None:
     peak_terms = sfu.value / 1e9          # G sincos pairs per second
     ach1 = s1_eval / (k1_ms * 1e-3) / 1e9
     ach2 = s2_eval / (k2_ms * 1e-3) / 1e9
-    traffic = traffic_from_profiles("k_stage1", WORKLOAD["workload"])
+    traffic = traffic_from_profiles("k_stage1", workload["workload"])
     roofline = {"bound": "sfu", "kernel": "k_stage1", "achieved": ach1, "peak": peak_terms, "unit": "Gterm/s",
                 "frac": ach1 / peak_terms, "traffic": traffic,
                 "peak_source": "measured on this GPU by vb_measure_peaks (sin+cos pairs/s, MUFU)",
@@ -853,7 +862,7 @@ def main() -> None:
 
     out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
-           "vs_baseline": None, "dtype": "f32+f64phase", "data": "synthetic", "config": WORKLOAD,
+           "vs_baseline": None, "dtype": "f32+f64phase", "data": "synthetic", "config": workload,
            "run": {"parallelism": f"replicas{ws}", "kernel_shape": shape, "shapes": shape_info,
                    "terms_per_step": terms_step, "stage1_terms": r["stage1_terms"],
                    "stage2_terms": r["stage2_terms"], "groups": r["groups_total"], "n_half": p.n_half,

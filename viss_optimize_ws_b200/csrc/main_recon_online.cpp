@@ -296,8 +296,15 @@ int main(int argc, char** argv) {
   cfg.use_graph = use_graph;
   cfg.device = 0;
 
+  // --report_json: the SFU (sin + cos) rate of this GPU, measured once, is the
+  // denominator of the per-stage roofline fractions of each day
+  double sfu_pairs = 0.0;
+  if (!report_json.empty()) {
+    double f32 = 0, f64 = 0, clk = 0;
+    if (vb_measure_peaks(&sfu_pairs, &f32, &f64, &clk) != VB_OK) sfu_pairs = 0.0;
+  }
   std::ostringstream json;
-  json << "{\"days\": [";
+  json << "{\"sfu_pairs_per_s\": " << sfu_pairs << ", \"days\": [";
   // one run context for all days: each further day only swaps the orbit
   vbtext::AsyncWriter writer(async_write != 0);
   vb_pipeline* p = nullptr;
@@ -545,7 +552,17 @@ int main(int argc, char** argv) {
     json << (di ? ", " : "") << "{\"day\": " << dayid << ", \"t_stage1_ms\": " << rep.t_stage1_ms
          << ", \"t_stage2_ms\": " << rep.t_stage2_ms << ", \"stage1_terms\": " << rep.stage1_terms
          << ", \"stage2_terms\": " << rep.stage2_terms << ", \"groups\": " << rep.groups_total
-         << ", \"error_flags\": " << rep.error_flags << "}";
+         << ", \"error_flags\": " << rep.error_flags << ", \"t_s1_kernel_ms\": " << rep.t_s1_kernel_ms
+         << ", \"t_s2_kernel_ms\": " << rep.t_s2_kernel_ms << ", \"s1_counters\": [" << rep.s1_counters[0] << ", "
+         << rep.s1_counters[1] << ", " << rep.s1_counters[2] << ", " << rep.s1_counters[3]
+         << "], \"s2_counters\": [" << rep.s2_counters[0] << ", " << rep.s2_counters[1] << ", "
+         << rep.s2_counters[2] << ", " << rep.s2_counters[3] << "]";
+    // evaluated terms (visible-fast + masked) per second over the kernel time, against the SFU rate
+    auto frac = [&](const unsigned long long* c, double ms) {
+      return (sfu_pairs > 0 && ms > 0) ? (double)(c[0] + c[1]) / (ms * 1e-3) / sfu_pairs : 0.0;
+    };
+    json << ", \"stage1_sfu_frac\": " << frac(rep.s1_counters, rep.t_s1_kernel_ms)
+         << ", \"stage2_sfu_frac\": " << frac(rep.s2_counters, rep.t_s2_kernel_ms) << "}";
   }
   if (p) vb_pipeline_destroy(p);
   if (d_acc) vb_free(d_acc);

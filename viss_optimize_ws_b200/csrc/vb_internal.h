@@ -47,17 +47,20 @@ struct Stage1Plan {
   int precision, cull, phase_corrected, blockage;
   int bpt, minb, stage_pix, chunk_pix, cull_tile, refine_pix;
   int mask_visible;   // tile-cone: tiles proven visible still take the per-pixel test
+  int pair_blk;       // pixels of a ring-pairing block (power of two dividing every processed range)
   int64_t npix;
+  int64_t npix_pad;   // npix rounded up to a whole pairing block (pad pixels have B = 0)
   int n_half, nbl;
   int nchunk, n_btile, n_items, grid;
   int ntile_cull;
   double max_turns;
 };
 
+struct PixPair;               // two staged pixels (vb_stage1.cu)
 struct Stage1Buffers {       // slices of a workspace
-  double2* lm = nullptr;
-  float4* nb = nullptr;
-  float4* f4 = nullptr;
+  PixPair* pairs = nullptr;  // [npix_pad / 2], ring-paired order within each pairing block
+  float4* f4 = nullptr;      // [npix_pad] (l, m, n, B) in the same order
+  int* pair_shared = nullptr;  // [npix_pad / pair_blk]: leading pairs of each block whose pixels share n
   ExactCone* cones = nullptr;
   ExactCone* subcones = nullptr;   // tile-cone refinement sub-tiles
   double2* partial = nullptr;
@@ -87,10 +90,7 @@ struct Stage2Plan {
   int nchunk_target;    // group chunks per pixel block (upper bound; sizes the partials)
   size_t cub_sort_bytes, cub_scan_bytes;
 };
-struct Stage2Pixels {       // pixel records already packed by the caller
-  const double2* lm = nullptr;
-  const float4* nb = nullptr;
-  const float4* f4 = nullptr;
+struct Stage2Pixels {       // per-pixel state the caller already prepared
   bool cones_ready = false;  // block cones already computed in this workspace
 };
 int stage2_plan(int n_half_total, int nseg, int64_t npix, const vb_stage2_opts* o, Stage2Plan* p);

@@ -554,9 +554,6 @@ static int enqueue_stages(vb_pipeline* p) {
   if (rc != VB_OK) return rc;
   VB_CUDA(ew);
   Stage2Pixels pre;
-  pre.lm = p->b1.lm;
-  pre.nb = p->b1.nb;
-  pre.f4 = p->b1.f4;
   pre.cones_ready = p->s2_cones_ready;
   VB_TRY(stage2_finish(&sky, &bl, p->Vh, p->nseg, p->p2, p->ws2, p->ws2_bytes, gr, p->C, p->W, p->segp,
                        p->counters + 4, p->wsum, p->s, &pre, p->ev[7], p->ev[8]));
@@ -864,6 +861,7 @@ extern "C" int vb_pipeline_device_ptr(vb_pipeline* p, const char* name, void** p
       {"nm1", p->nm1, p->nres}, {"cx", p->cx, p->ntile}, {"cy", p->cy, p->ntile}, {"cz", p->cz, p->ntile},
       {"cosA", p->cosA, p->ntile}, {"sinA", p->sinA, p->ntile}, {"seg_t0", p->d_t0, p->nseg},
       {"seg_tlen", p->d_tlen, p->nseg}, {"seg_params", p->segp, p->nseg},
+      {"pair_shared", p->b1.pair_shared, p->p1.pair_blk > 0 ? p->p1.npix_pad / p->p1.pair_blk : 0},
   };
   for (const E& e : tab)
     if (std::strcmp(e.k, name) == 0) {

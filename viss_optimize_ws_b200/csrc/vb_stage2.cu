@@ -40,7 +40,8 @@ struct GroupRec {         // 96 bytes
   float cp1, cp2;         // horizon cosines of the representative endpoints
   float4 p1, p2;          // (x, y, z, invn) of the representative endpoints
   float chi, clo;         // c split into two floats (double-single phase)
-  int key, flags;         // flags: bit0 = skip (key 0 / nothing to add)
+  int key, flags;         // flags: bit0 = skip (key 0 / nothing to add), bit1 = non-finite V,
+                          // bits 2.. = segment
 };
 struct GroupMeta {        // members of a group (member-sampling path)
   int s0, L, seg, pad;
@@ -241,7 +242,7 @@ __global__ void k_group_records(const RecArgs r, int max_groups) {
     const vb_seg_params q = r.sp[seg];
     GroupRec o;
     o.key = key;
-    o.flags = (key == 0) ? 1 : 0;
+    o.flags = ((key == 0) ? 1 : 0) | (seg << 2);
     float ugu = 0.f, vgu = 0.f;
     if (key != 0) {
       int tmp = key - 1;
@@ -300,14 +301,13 @@ __host__ __device__ inline int group_chunk(int ng, int nchunk_target) {
 }
 
 struct ReconArgs {
-  const float4* f4;          // (l, m, n, B) per pixel
-  const double2* lm;
-  const float4* nb;          // (n as FP64 bits, B, nm1)
+  const float *l, *m, *n;    // the sky's direction cosines (FP64 phases take their exact doubles)
   int64_t npix;
   int block_pix, nblocks, nchunk_target;
   const int* ngroups;
   const GroupRec* rec;
   const GroupMeta* meta;
+  const vb_seg_params* sp;   // per segment: fa, fb, first group, group count
   const int* svals;
   const float* V;
   const float *x1, *y1, *z1, *in1, *x2, *y2, *z2, *in2, *cp1, *cp2;
@@ -464,6 +464,66 @@ __device__ __forceinline__ void rec_term(const TermRec<MODE>& r, const RecPix& p
   }
 }
 
+// FP32 with FP64 phase, and FP64: the phase of a (group, pixel) term is
+// a l' + b m' with the segment's l' = l + fa n, m' = m + fb n (the upstream
+// form, viss_recon_kernel.cuh:620-626), formed in FP64 once per pixel per stage
+// because the stages of k_recon_rec hold the groups of one segment: two FP64
+// products per term instead of three.  Two groups share a 48-byte record (the
+// dither pair): three shared loads per two groups.
+template <int MODE>
+__device__ constexpr bool rec_pairs() {
+  return MODE == VB_PREC_FP32_FP64PH || MODE == VB_PREC_FP64;
+}
+struct PairRec {
+  double2 ab0, ab1;   // (a, b) of the even and of the odd slot
+  float4 v;           // (vx, -vy) of the even slot, then of the odd slot (dither signs applied)
+};
+
+template <int MODE, int PAR, class Acc>
+__device__ __forceinline__ void pair_term(const double2 ab, const float vx, const float nvy, const double lp,
+                                          const double mp, Acc& acc) {
+  if constexpr (MODE == VB_PREC_FP32_FP64PH) {
+    constexpr double K = kMagic2 + (PAR ? 0.5 : 0.0);
+    const double t = fma(ab.x, lp, fma(ab.y, mp, K));
+    const unsigned lo = (unsigned)__double2loint(t);
+    const unsigned kb = (lo & 0x7FFFFFu) | 0x4B000000u;
+    const float ang = __fmaf_rn(__uint_as_float(kb), kAngScale2, -kTwoPiF2);
+    float s, c;
+    __sincosf(ang, &s, &c);
+    acc = fmaf(vx, c, acc);
+    acc = fmaf(nvy, s, acc);
+  } else {
+    const double t = fma(ab.x, lp, ab.y * mp);
+    double s, c;
+    sincospi(2.0 * t, &s, &c);
+    acc = fma((double)vx, c, acc);
+    acc = fma((double)nvy, s, acc);
+  }
+}
+
+// Writes group record g into slot k of a stage list (pair records or term records).
+template <int MODE, class L>
+__device__ __forceinline__ void put_term(L* list, int k, const GroupRec& g) {
+  const TermRec<MODE> t = make_term<MODE>(g, k & 1);
+  if constexpr (rec_pairs<MODE>()) {
+    PairRec& pr = list[k >> 1];
+    if (k & 1) { pr.ab1 = make_double2(t.a, t.b); pr.v.z = t.vx; pr.v.w = t.nvy; }
+    else { pr.ab0 = make_double2(t.a, t.b); pr.v.x = t.vx; pr.v.y = t.nvy; }
+  } else {
+    list[k] = t;
+  }
+}
+template <int MODE, class L>
+__device__ __forceinline__ void put_zero(L* list, int k) {
+  if constexpr (rec_pairs<MODE>()) {
+    PairRec& pr = list[k >> 1];
+    if (k & 1) { pr.ab1 = make_double2(0.0, 0.0); pr.v.z = 0.f; pr.v.w = 0.f; }
+    else { pr.ab0 = make_double2(0.0, 0.0); pr.v.x = 0.f; pr.v.y = 0.f; }
+  } else {
+    list[k] = zero_term<MODE>();
+  }
+}
+
 // Exact-cone class of a representative against a pixel block (0 hidden,
 // 1 visible, 2 mixed).  Out of line: it runs once per (group, block) and would
 // otherwise take registers from the term loop.
@@ -477,17 +537,21 @@ __device__ __noinline__ int exact_group_class(const ExactCone* cone, float4 p1, 
 // occ_mode 2 (representative) and blockage=0 (group averages) paths.
 //
 // Work item = (pixel block of PPT * 256 pixels, chunk of groups).  Each thread
-// owns PPT pixels.  Per stage of up to 256 groups the CTA classifies every
-// group against the block (hidden / visible / mixed; exact cones with
-// VB_CULL_EXACT, otherwise mixed) and compacts the visible and the mixed ones
-// into two lists in shared memory; the term loop then runs without branches
-// over the visible list and with the per-pixel occlusion test over the mixed
-// list, two groups (the dither pair) by PPT pixels per step.
+// owns PPT pixels.  The chunk is walked in stages of up to 256 groups that
+// belong to one segment; per stage the CTA classifies every group against the
+// block (hidden / visible / mixed; exact cones with VB_CULL_EXACT, otherwise
+// mixed) and compacts the visible and the mixed ones into two lists in shared
+// memory; the term loop then runs without branches over the visible list and
+// with the per-pixel occlusion test over the mixed list, two groups (the
+// dither pair) by PPT pixels per step.
 template <int MODE, int PPT>
 __global__ void __launch_bounds__(S2_THREADS, 2) k_recon_rec(const ReconArgs a) {
   constexpr int NW = S2_THREADS / 32;
-  __shared__ TermRec<MODE> s_vis[S2_STAGE + 1];
-  __shared__ TermRec<MODE> s_mix[S2_STAGE + 1];
+  constexpr bool kPairs = rec_pairs<MODE>();
+  using ListT = typename std::conditional<kPairs, PairRec, TermRec<MODE>>::type;
+  constexpr int kListLen = kPairs ? (S2_STAGE / 2 + 1) : (S2_STAGE + 1);
+  __shared__ ListT s_vis[kListLen];
+  __shared__ ListT s_mix[kListLen];
   __shared__ OccRec s_occ[S2_STAGE + 1];
   __shared__ int s_wv[NW], s_wm[NW];
   __shared__ int s_item;
@@ -522,10 +586,8 @@ __global__ void __launch_bounds__(S2_THREADS, 2) k_recon_rec(const ReconArgs a) 
       act[q] = pix < a.npix;
       px[q] = RecPix{0.0, 0.0, 0.0, 0.f, 0.f, 0.f};
       if (act[q]) {
-        const float4 f = a.f4[pix];
-        const double2 lm = a.lm[pix];
-        const float4 nbr = a.nb[pix];
-        px[q] = RecPix{lm.x, lm.y, __hiloint2double(__float_as_int(nbr.y), __float_as_int(nbr.x)), f.x, f.y, f.z};
+        px[q].lf = a.l[pix]; px[q].mf = a.m[pix]; px[q].nf = a.n[pix];
+        px[q].ld = px[q].lf; px[q].md = px[q].mf; px[q].nd = px[q].nf;
       }
     }
     double totC[PPT];
@@ -536,8 +598,13 @@ __global__ void __launch_bounds__(S2_THREADS, 2) k_recon_rec(const ReconArgs a) 
 
     const int g_begin = gc * gchunk;
     const int g_end = min(ng, g_begin + gchunk);
-    for (int gs = g_begin; gs < g_end; gs += S2_STAGE) {
-      const int nst = min(S2_STAGE, g_end - gs);
+    int gs = g_begin;
+    while (gs < g_end) {
+      // this stage: up to 256 groups of the segment that group gs belongs to
+      // (every thread reads the same words)
+      const int seg = a.rec[gs].flags >> 2;
+      const int seg_end = a.sp[seg].group_start + a.sp[seg].nuniq;
+      const int nst = min(S2_STAGE, min(g_end, seg_end) - gs);
       __syncthreads();   // previous stage's lists fully read; s_cone visible
       // --- classify this stage's groups and compact them ---------------------
       int cls = 0;
@@ -566,18 +633,17 @@ __global__ void __launch_bounds__(S2_THREADS, 2) k_recon_rec(const ReconArgs a) 
       }
       const unsigned below = (1u << lane) - 1u;
       if (cls == 1) {
-        const int k = ov + __popc(bv & below);
-        s_vis[k] = make_term<MODE>(r, k & 1);
+        put_term<MODE>(s_vis, ov + __popc(bv & below), r);
       } else if (cls == 2) {
         const int k = om + __popc(bm & below);
-        s_mix[k] = make_term<MODE>(r, k & 1);
+        put_term<MODE>(s_mix, k, r);
         s_occ[k] = OccRec{r.p1, r.p2, r.cp1, r.cp2};
       }
       if (threadIdx.x == 0) {
         // pad odd lists with a record that adds nothing (and fails the test)
-        if (nv & 1) s_vis[nv] = zero_term<MODE>();
+        if (nv & 1) put_zero<MODE>(s_vis, nv);
         if (nm & 1) {
-          s_mix[nm] = zero_term<MODE>();
+          put_zero<MODE>(s_mix, nm);
           s_occ[nm] = OccRec{make_float4(0.f, 0.f, 0.f, 0.f), make_float4(0.f, 0.f, 0.f, 0.f), INFINITY, INFINITY};
         }
         c_fast += (unsigned long long)nv * npx_blk;
@@ -585,19 +651,46 @@ __global__ void __launch_bounds__(S2_THREADS, 2) k_recon_rec(const ReconArgs a) 
         c_hid += (unsigned long long)(nst - nv - nm) * npx_blk;
         c_all += (unsigned long long)nst * npx_blk;
       }
+      // the segment's coordinates l' = l + fa n, m' = m + fb n of this thread's pixels
+      double lp[PPT], mp[PPT];
+      if constexpr (kPairs) {
+        const double fa = (double)a.sp[seg].fa, fb = (double)a.sp[seg].fb;
+#pragma unroll
+        for (int q = 0; q < PPT; ++q) {
+          lp[q] = mp[q] = 0.0;
+          if (act[q]) {
+            // the exact doubles of the float coordinates (the float registers
+            // stay for the occlusion test)
+            const double nd = (double)px[q].nf;
+            lp[q] = fma(fa, nd, (double)px[q].lf);
+            mp[q] = fma(fb, nd, (double)px[q].mf);
+          }
+        }
+      }
       __syncthreads();
 
       // --- visible groups: no test ---------------------------------------------
       Acc e[PPT], o[PPT];
 #pragma unroll
       for (int q = 0; q < PPT; ++q) { e[q] = Acc(0); o[q] = Acc(0); }
-      for (int k = 0; k < nv; k += 2) {
-        const TermRec<MODE> r0 = s_vis[k];
-        const TermRec<MODE> r1 = s_vis[k + 1];
+      if constexpr (kPairs) {
+        for (int k2 = 0; k2 < nv; k2 += 2) {
+          const PairRec pr = s_vis[k2 >> 1];
 #pragma unroll
-        for (int q = 0; q < PPT; ++q) {
-          rec_term<MODE, 0>(r0, px[q], e[q]);
-          rec_term<MODE, 1>(r1, px[q], o[q]);
+          for (int q = 0; q < PPT; ++q) {
+            pair_term<MODE, 0>(pr.ab0, pr.v.x, pr.v.y, lp[q], mp[q], e[q]);
+            pair_term<MODE, 1>(pr.ab1, pr.v.z, pr.v.w, lp[q], mp[q], o[q]);
+          }
+        }
+      } else {
+        for (int k = 0; k < nv; k += 2) {
+          const TermRec<MODE> r0 = s_vis[k];
+          const TermRec<MODE> r1 = s_vis[k + 1];
+#pragma unroll
+          for (int q = 0; q < PPT; ++q) {
+            rec_term<MODE, 0>(r0, px[q], e[q]);
+            rec_term<MODE, 1>(r1, px[q], o[q]);
+          }
         }
       }
       if (a.blockage) {
@@ -606,10 +699,16 @@ __global__ void __launch_bounds__(S2_THREADS, 2) k_recon_rec(const ReconArgs a) 
       }
       // --- mixed groups: per-pixel occlusion test ------------------------------
       for (int k = 0; k < nm; k += 2) {
-        const TermRec<MODE> r0 = s_mix[k];
-        const TermRec<MODE> r1 = s_mix[k + 1];
         const OccRec c0 = s_occ[k];
         const OccRec c1 = s_occ[k + 1];
+        PairRec pr;
+        TermRec<MODE> r0, r1;
+        if constexpr (kPairs) {
+          pr = s_mix[k >> 1];
+        } else {
+          r0 = s_mix[k];
+          r1 = s_mix[k + 1];
+        }
 #pragma unroll
         for (int q = 0; q < PPT; ++q) {
           const RecPix& p = px[q];
@@ -618,8 +717,13 @@ __global__ void __launch_bounds__(S2_THREADS, 2) k_recon_rec(const ReconArgs a) 
           const bool in1 = occ_dot(p.lf, p.mf, p.nf, c1.p1.x, c1.p1.y, c1.p1.z, c1.p1.w) >= c1.cp1 &&
                            occ_dot(p.lf, p.mf, p.nf, c1.p2.x, c1.p2.y, c1.p2.z, c1.p2.w) >= c1.cp2;
           Acc t0 = Acc(0), t1 = Acc(0);
-          rec_term<MODE, 0>(r0, p, t0);
-          rec_term<MODE, 1>(r1, p, t1);
+          if constexpr (kPairs) {
+            pair_term<MODE, 0>(pr.ab0, pr.v.x, pr.v.y, lp[q], mp[q], t0);
+            pair_term<MODE, 1>(pr.ab1, pr.v.z, pr.v.w, lp[q], mp[q], t1);
+          } else {
+            rec_term<MODE, 0>(r0, p, t0);
+            rec_term<MODE, 1>(r1, p, t1);
+          }
           e[q] += in0 ? t0 : Acc(0);
           o[q] += in1 ? t1 : Acc(0);
           totW[q] += (in0 ? 1u : 0u) + (in1 ? 1u : 0u);
@@ -641,6 +745,7 @@ __global__ void __launch_bounds__(S2_THREADS, 2) k_recon_rec(const ReconArgs a) 
           totC[q] += (double)e[q] + (double)o[q];
         }
       }
+      gs += nst;
     }
 #pragma unroll
     for (int q = 0; q < PPT; ++q) {
@@ -684,12 +789,8 @@ __global__ void __launch_bounds__(S2_THREADS) k_recon_members(const ReconArgs a)
     float lf = 0.f, mf = 0.f, nf = 0.f;
     double ld = 0.0, md = 0.0, nd = 0.0;
     if (active) {
-      const float4 f = a.f4[pix];
-      lf = f.x; mf = f.y; nf = f.z;
-      const double2 lm = a.lm[pix];
-      const float4 nbr = a.nb[pix];
-      ld = lm.x; md = lm.y;
-      nd = __hiloint2double(__float_as_int(nbr.y), __float_as_int(nbr.x));
+      lf = a.l[pix]; mf = a.m[pix]; nf = a.n[pix];
+      ld = lf; md = mf; nd = nf;
     }
     const int npx_blk = (int)min((int64_t)a.block_pix, a.npix - (int64_t)blk * a.block_pix);
     double totC = 0.0;
@@ -851,9 +952,6 @@ struct S2Slices {
   double* Cpart;
   unsigned* Wpart;
   ExactCone* cones;
-  double2* lm;
-  float4* nb;
-  float4* f4;
   float* Vfull;
   void* cub_sort;
   void* cub_scan;
@@ -881,9 +979,6 @@ static size_t carve2(const Stage2Plan& p, void* ws, size_t cap, S2Slices* s) {
   x.Cpart = c.take<double>((size_t)p.nchunk_target * (size_t)p.npix);
   x.Wpart = c.take<unsigned>((size_t)p.nchunk_target * (size_t)p.npix);
   x.cones = c.take<ExactCone>(p.nblocks);
-  x.lm = c.take<double2>(p.npix);
-  x.nb = c.take<float4>(p.npix);
-  x.f4 = c.take<float4>(p.npix);
   x.Vfull = p.mirror ? nullptr : c.take<float>((size_t)4 * (p.n_half_total > 0 ? p.n_half_total : 1));
   x.cub_sort = c.take<char>(p.cub_sort_bytes);
   x.cub_scan = c.take<char>(p.cub_scan_bytes);
@@ -1015,23 +1110,15 @@ int stage2_finish(const vb_sky* sky, const vb_baselines* bl, const float* V_half
     k_group_records<<<g, 256, 0, st>>>(r, n);
     VB_LAUNCH_CHECK();
   }
-  // 7. pixel records and block cones (unless the caller already holds them)
-  const double2* plm = x.lm;
-  const float4* pnb = x.nb;
-  const float4* pf4 = x.f4;
-  if (pre && pre->lm) {
-    plm = pre->lm; pnb = pre->nb; pf4 = pre->f4;
-  } else {
-    VB_TRY(geom_pack_pixels(sky->B, sky->l, sky->m, sky->n, p.npix, x.lm, x.nb, x.f4, st));
-  }
+  // 7. block cones (unless the caller already holds them)
   if (p.cull == VB_CULL_EXACT && !(pre && pre->cones_ready))
     VB_TRY(geom_exact_cones(p.block_pix, sky->l, sky->m, sky->n, p.npix, x.cones, st));
   // 8. reconstruction over (pixel block x group chunk)
   if (n > 0) {
     ReconArgs ra{};
-    ra.f4 = pf4; ra.lm = plm; ra.nb = pnb; ra.npix = p.npix;
+    ra.l = sky->l; ra.m = sky->m; ra.n = sky->n; ra.npix = p.npix;
     ra.block_pix = p.block_pix; ra.nblocks = p.nblocks; ra.nchunk_target = p.nchunk_target;
-    ra.ngroups = x.ngroups; ra.rec = x.rec; ra.meta = x.meta; ra.svals = sv; ra.V = Vk;
+    ra.ngroups = x.ngroups; ra.rec = x.rec; ra.meta = x.meta; ra.sp = x.sp; ra.svals = sv; ra.V = Vk;
     ra.x1 = bl->x1; ra.y1 = bl->y1; ra.z1 = bl->z1; ra.in1 = bl->invn1;
     ra.x2 = bl->x2; ra.y2 = bl->y2; ra.z2 = bl->z2; ra.in2 = bl->invn2;
     ra.cp1 = bl->cosphi1; ra.cp2 = bl->cosphi2; ra.cosphi = bl->cosphi;
