@@ -357,19 +357,13 @@ def test_library_kernel_masks_match_upstream(case, vb, ref, cull):
 def test_tilecone_subtile_refinement_is_bit_identical(case, vb, prec):
     """Exact sub-tiles inside tile-cone mixed tiles change only which path a
     warp takes (skip / class select / per-pixel test): V is bit-identical with
-    refinement off for 128-pixel sub-tiles (the default), and the counters move
-    terms from masked to fast / hidden.  Sub-tiles of 32 or 64 pixels also set
-    the ring-pairing block, so the FP32 sums run in another pixel order: equal
-    to summation rounding."""
+    refinement off, and the counters move terms from masked to fast / hidden."""
     sky, bl = structs(case)
     pm = {"fp64": vb.PREC_FP64, "fp32_fp64phase": vb.PREC_FP32_FP64PH, "fp32_dsphase": vb.PREC_FP32_DSPH}[prec]
     Voff, coff = stage1(sky, bl, precision=pm, cull=vb.CULL_TILECONE, refine_pix=-1)
     for r in (0, 32, 64, 128):
         V, c = stage1(sky, bl, precision=pm, cull=vb.CULL_TILECONE, refine_pix=r)
-        if r in (0, 128):
-            assert np.array_equal(V.view(np.uint64), Voff.view(np.uint64)), r
-        else:
-            assert rel_err(V, Voff)[0] < 1e-6, r
+        assert np.array_equal(V.view(np.uint64), Voff.view(np.uint64)), r
         assert c[3] == coff[3] and c[1] <= coff[1] and c[0] >= coff[0] and c[2] >= coff[2]
 
 
@@ -402,12 +396,11 @@ def test_device_error_word_in_the_workspace(vb, case):
 
 
 @pytest.mark.parametrize("prec", ["fp32_fp64phase", "fp64"])
-def test_ring_pairing_on_a_non_healpix_sky(case, vb, orc, prec):
-    """Stage 1 pairs the pixels of one HEALPix ring so that a pair shares its
-    w n product, after checking bit for bit that both n are equal.  On the
-    same pixels in a shuffled order (no rings left) every pair is summed with
-    its own n: the sums still match the FP64 oracle on the shuffled arrays, and
-    the term counters are those of the ordered sky."""
+def test_stage1_on_a_shuffled_pixel_order(case, vb, orc, prec):
+    """The C-ABI stage 1 takes any pixel arrays, not only HEALPix NEST order:
+    the same pixels in a shuffled order (cull tiles then hold scattered
+    pixels) match the FP64 oracle on the shuffled arrays, and the term
+    counters are those of the ordered sky."""
     c = case
     rng = np.random.default_rng(5)
     perm = rng.permutation(c["npix"])
@@ -424,18 +417,3 @@ def test_ring_pairing_on_a_non_healpix_sky(case, vb, orc, prec):
     sky0, _ = structs(c, tile=False)
     V0, cnt0 = stage1(sky0, bl, precision=pm, cull=vb.CULL_NONE)
     assert np.array_equal(cnt, cnt0)
-
-
-def test_ring_pairs_found_on_healpix_skies(gpu, vb):
-    """On a HEALPix sky every 128-pixel block yields its 60 ring pairs (the
-    pixels of a ring carry bit-identical n), so 93.75 % of the pixels share
-    their w n product with their partner."""
-    kw = dict(nside=256, orbit_model=vb.ORBIT_SYNTHETIC, nsat=4, tsteps=8, segs=2, lambda_m=30.0, occ_R_m=6371e3,
-              cull="tilecone", viss_tile_pix=1024, mirror=1, grid_res=65, bl_max_m=0.0)
-    with vb.Pipeline(vb.run_config(**kw)) as p:
-        p.set_sky(vb.synthetic_sky(256, seed=1))
-        p.make_baselines()
-        p.run()
-        shared = p.get("pair_shared").view(np.int32)
-    assert shared.size == 12 * 256 * 256 // 128
-    assert np.all(shared == 60), np.unique(shared)

@@ -42,28 +42,6 @@ def test_nest_integer_parts(orc):
             assert cnt == 4 * int(nr[jr == r][0])
 
 
-def test_ring_pairing_premise(orc):
-    """Within an aligned block of 2^k <= nside^2 NEST-consecutive pixels, the
-    pixels with equal in-block x + y (x = the even bits, y = the odd bits of
-    the index within the block) lie on one ring, whose z (and n) the ring
-    alone sets: the premise of stage 1's ring pairs."""
-    def bits(v, start):
-        out = np.zeros_like(v)
-        for b in range(8):
-            out |= ((v >> (2 * b + start)) & 1) << b
-        return out
-    for nside in (16, 64):
-        face, ix, iy, jr, nr, ks, jp = orc.nest_ints(nside)
-        npix = 12 * nside * nside
-        idx = np.arange(npix, dtype=np.int64)
-        for bp in (32, 64, 128):
-            loc = idx % bp
-            d = bits(loc, 0) + bits(loc, 1)
-            key = (idx // bp) * 64 + d
-            pairs = np.unique(np.stack([key, jr.astype(np.int64)]), axis=1)
-            assert pairs.shape[1] == np.unique(key).size, (nside, bp)
-
-
 def test_lmn_unit_and_equal_area(orc):
     nside = 32
     l, m, n = orc.nest_lmn_f64(nside)

@@ -128,7 +128,7 @@ class Pipeline:
 
     def get(self, name: str) -> np.ndarray:
         dt = {"C": np.float32, "W": np.uint32, "V_half_d": np.float64, "seg_t0": np.int32,
-              "seg_tlen": np.int32, "pair_shared": np.int32}.get(name, np.float32)
+              "seg_tlen": np.int32}.get(name, np.float32)
         p, n = self.ptr(name)
         if not p or n == 0:
             return np.empty(0, dtype=dt)

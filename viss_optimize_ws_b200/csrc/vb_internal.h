@@ -47,20 +47,17 @@ struct Stage1Plan {
   int precision, cull, phase_corrected, blockage;
   int bpt, minb, stage_pix, chunk_pix, cull_tile, refine_pix;
   int mask_visible;   // tile-cone: tiles proven visible still take the per-pixel test
-  int pair_blk;       // pixels of a ring-pairing block (power of two dividing every processed range)
   int64_t npix;
-  int64_t npix_pad;   // npix rounded up to a whole pairing block (pad pixels have B = 0)
   int n_half, nbl;
   int nchunk, n_btile, n_items, grid;
   int ntile_cull;
   double max_turns;
 };
 
-struct PixPair;               // two staged pixels (vb_stage1.cu)
 struct Stage1Buffers {       // slices of a workspace
-  PixPair* pairs = nullptr;  // [npix_pad / 2], ring-paired order within each pairing block
-  float4* f4 = nullptr;      // [npix_pad] (l, m, n, B) in the same order
-  int* pair_shared = nullptr;  // [npix_pad / pair_blk]: leading pairs of each block whose pixels share n
+  double2* lm = nullptr;
+  float4* nb = nullptr;
+  float4* f4 = nullptr;
   ExactCone* cones = nullptr;
   ExactCone* subcones = nullptr;   // tile-cone refinement sub-tiles
   double2* partial = nullptr;

@@ -861,7 +861,6 @@ extern "C" int vb_pipeline_device_ptr(vb_pipeline* p, const char* name, void** p
       {"nm1", p->nm1, p->nres}, {"cx", p->cx, p->ntile}, {"cy", p->cy, p->ntile}, {"cz", p->cz, p->ntile},
       {"cosA", p->cosA, p->ntile}, {"sinA", p->sinA, p->ntile}, {"seg_t0", p->d_t0, p->nseg},
       {"seg_tlen", p->d_tlen, p->nseg}, {"seg_params", p->segp, p->nseg},
-      {"pair_shared", p->b1.pair_shared, p->p1.pair_blk > 0 ? p->p1.npix_pad / p->p1.pair_blk : 0},
   };
   for (const E& e : tab)
     if (std::strcmp(e.k, name) == 0) {

@@ -28,7 +28,6 @@
 #include <cmath>
 #include <algorithm>
 #include <type_traits>
-#include <vector>
 
 #include "vb_common.cuh"
 #include "vb_geom.cuh"
@@ -45,36 +44,6 @@ constexpr int kCullTileconeMV = 3;
 template <int CULL>
 __host__ __device__ constexpr bool is_tilecone() { return CULL == VB_CULL_TILECONE || CULL == kCullTileconeMV; }
 
-// Two staged pixels, the even and the odd slot of a dither pair: FP64 (l, m)
-// of each, n of the even slot with both brightnesses, n of the odd slot.
-// Within each pairing block (pair_blk NEST-consecutive pixels) the pixels are
-// reordered so that the leading pairs hold two pixels of one HEALPix ring:
-// their n is the same float (it depends on the ring alone), so a pair's w n
-// product is formed once for both.  pair_shared[block] counts those leading
-// pairs; each was checked bit for bit when packed, so any sky is summed
-// correctly and only the saving depends on the HEALPix layout.
-struct __align__(16) PixPair {
-  double2 lm0, lm1;
-  double n0;
-  float B0, B1;
-  double n1;
-  float pad0, pad1;
-};
-
-// Largest pairing block: 128 NEST pixels = 16 x 8 in face coordinates,
-// 23 rings, 60 shared pairs and 4 mixed ones.
-constexpr int kPairBlkMax = 128;
-
-// Pairing order of a block of bp NEST-consecutive pixels (bp a power of two):
-// src[j] = local index of the pixel in slot j.  Pixels of a ring (one value
-// of x + y in the block's face coordinates) are paired first, in ring order;
-// the leftovers of odd rings follow in consecutive pairs.  Returns the number
-// of ring pairs.
-struct PairOrder {
-  int bp, shared;
-  short src[kPairBlkMax];
-};
-
 // F32X phase reduction: magic = 1.5 * 2^29 keeps every partial sum of the FMA
 // chain in [2^29, 2^30) (|u| + |v| + |w| < 2^28); the double's ulp is then
 // 2^-23 turns, so each FMA rounds to nearest on the 2^-23-turn grid the FP32
@@ -86,11 +55,10 @@ constexpr float kAngScale = 6.28318530717958647692f * 1.1920928955078125e-7f;  /
 constexpr double kMaxUvwF32X = 67108864.0;         // 2^26: 3 * 2^26 < 2^28
 
 struct S1Args {
-  const PixPair* __restrict__ pairs;
+  const double2* __restrict__ lm;
+  const float4* __restrict__ nb;
   const float4* __restrict__ f4;
-  const int* __restrict__ pair_shared;
-  int64_t npix, npix_pad;
-  int pair_blk;
+  int64_t npix;
   int cull, cull_tile, stage_pix, chunk_pix, nchunk, n_btile, n_items;
   const float *tcx, *tcy, *tcz, *tcosA, *tsinA;   // VB_CULL_TILECONE
   const ExactCone* cones;                          // VB_CULL_EXACT
@@ -106,42 +74,24 @@ struct S1Args {
   unsigned* err;
 };
 
+// one staged pixel: FP64 (l, m), (n as two words, B, n - 1), FP32 (l, m, n, B);
+// interleaved so that a pixel's loads share one address with fixed offsets
+struct __align__(16) PixRec {
+  double2 lm;
+  float4 nb;
+  float4 f4;
+};
 
-// Phase data of one half-baseline, held in registers by the thread that owns it.
-struct BPhase {
+struct Baseline {
   double U, V, W, C;
   float uf, vf, wf, fw;   // FP32 copies; fw = -frac(w) (raw phase, DS)
   float ku, kv, kw;       // REF32: -2 pi * (u, v, w)
+  float x1, y1, z1, i1, x2, y2, z2, i2, c1, c2;
+  float ux1, uy1, uz1, ux2, uy2, uz2;
   int cls;    // class the pixel loop uses (tile class, or the sub-tile class when refined)
   int tcls;   // tile class (decides whether the staged partials are kept)
   bool active;
 };
-
-// Occlusion data of one half-baseline's two endpoints: positions, inverse
-// norms and horizon cosines.  Needed only by the tile / sub-tile tests and the
-// per-pixel test, so the kernel keeps it in shared memory (field-major, one
-// word per thread, so that each lane reads its own bank) and loads it where
-// it is used: registers stay free for the phase data of more baselines.
-struct Ends {
-  float x1, y1, z1, i1, c1, x2, y2, z2, i2, c2;
-};
-constexpr int kEndFields = 10;
-
-__device__ __forceinline__ void store_ends(float* s_ep, int k, const Ends& e) {
-  float* q = s_ep + k * kEndFields * S1_THREADS + threadIdx.x;
-  q[0 * S1_THREADS] = e.x1; q[1 * S1_THREADS] = e.y1; q[2 * S1_THREADS] = e.z1; q[3 * S1_THREADS] = e.i1;
-  q[4 * S1_THREADS] = e.c1; q[5 * S1_THREADS] = e.x2; q[6 * S1_THREADS] = e.y2; q[7 * S1_THREADS] = e.z2;
-  q[8 * S1_THREADS] = e.i2; q[9 * S1_THREADS] = e.c2;
-}
-
-__device__ __forceinline__ Ends load_ends(const float* s_ep, int k) {
-  const float* q = s_ep + k * kEndFields * S1_THREADS + threadIdx.x;
-  Ends e;
-  e.x1 = q[0 * S1_THREADS]; e.y1 = q[1 * S1_THREADS]; e.z1 = q[2 * S1_THREADS]; e.i1 = q[3 * S1_THREADS];
-  e.c1 = q[4 * S1_THREADS]; e.x2 = q[5 * S1_THREADS]; e.y2 = q[6 * S1_THREADS]; e.z2 = q[7 * S1_THREADS];
-  e.i2 = q[8 * S1_THREADS]; e.c2 = q[9 * S1_THREADS];
-  return e;
-}
 
 __device__ __forceinline__ float rint_magic(float x) {
   return __fsub_rn(__fadd_rn(x, 12582912.0f), 12582912.0f);
@@ -150,48 +100,47 @@ __device__ __forceinline__ float rint_magic(float x) {
 // VB_CULL_EXACT class of one baseline for one tile.  Kept out of line: the
 // FP64 cone test runs once per (baseline, tile), and inlining it into the
 // persistent kernel costs the pixel loop registers in every cull mode.
-__device__ __noinline__ int exact_tile_class(const ExactCone* cone, const Ends e) {
+__device__ __noinline__ int exact_tile_class(const ExactCone* cone, float x1, float y1, float z1, float i1, float c1,
+                                             float x2, float y2, float z2, float i2, float c2) {
   const ExactCone c = *cone;
-  const int e1 = exact_class(c, e.x1, e.y1, e.z1, e.i1, e.c1);
-  const int e2 = exact_class(c, e.x2, e.y2, e.z2, e.i2, e.c2);
+  const int e1 = exact_class(c, x1, y1, z1, i1, c1);
+  const int e2 = exact_class(c, x2, y2, z2, i2, c2);
   return (e1 < 0 || e2 < 0) ? kClsHid : ((e1 > 0 && e2 > 0) ? kClsVis : kClsMix);
 }
 
 // Tile class of one baseline for one cull tile (0 hidden, 1 visible, 2 mixed).
-// Upstream decision: ..._vissfast.cuh:519-531 (tile cone, with the unit
-// endpoint directions (x, y, z) * invn of ..._vissfast.cuh:484-485), per-pixel
-// mask everywhere for the plain kernel (viss_recon_kernel.cuh:270-274).  The
-// cull mode is a template argument so that each mode's kernel carries only its
-// own test.
+// Upstream decision: ..._vissfast.cuh:519-531 (tile cone), per-pixel mask
+// everywhere for the plain kernel (viss_recon_kernel.cuh:270-274).  The cull
+// mode is a template argument so that each mode's kernel carries only its own
+// test.
 template <int CULL>
-__device__ __forceinline__ int tile_class(const S1Args& a, const BPhase& b, const Ends& e, int tile_id) {
+__device__ __forceinline__ int tile_class(const S1Args& a, const Baseline& b, int tile_id) {
   if (!b.active) return kClsHid;
   if (!a.blockage) return kClsVis;
   if constexpr (is_tilecone<CULL>()) {
     const float cx = a.tcx[tile_id], cy = a.tcy[tile_id], cz = a.tcz[tile_id];
     const float cA = a.tcosA[tile_id], sA = a.tsinA[tile_id];
     bool vis1, hid1, vis2, hid2;
-    cone_classify(cone_dot(e.x1 * e.i1, e.y1 * e.i1, e.z1 * e.i1, cx, cy, cz), cA, sA, e.c1, vis1, hid1);
-    cone_classify(cone_dot(e.x2 * e.i2, e.y2 * e.i2, e.z2 * e.i2, cx, cy, cz), cA, sA, e.c2, vis2, hid2);
+    cone_classify(cone_dot(b.ux1, b.uy1, b.uz1, cx, cy, cz), cA, sA, b.c1, vis1, hid1);
+    cone_classify(cone_dot(b.ux2, b.uy2, b.uz2, cx, cy, cz), cA, sA, b.c2, vis2, hid2);
     return (hid1 || hid2) ? kClsHid : ((vis1 && vis2 && CULL != kCullTileconeMV) ? kClsVis : kClsMix);
   } else if constexpr (CULL == VB_CULL_EXACT) {
-    return exact_tile_class(a.cones + tile_id, e);
+    return exact_tile_class(a.cones + tile_id, b.x1, b.y1, b.z1, b.i1, b.c1, b.x2, b.y2, b.z2, b.i2, b.c2);
   } else {
     return kClsMix;
   }
 }
 
-__device__ __forceinline__ int tile_class_rt(const S1Args& a, const BPhase& b, const Ends& e, int tile_id) {
+__device__ __forceinline__ int tile_class_rt(const S1Args& a, const Baseline& b, int tile_id) {
   if (a.cull == VB_CULL_TILECONE)
-    return a.mask_visible ? tile_class<kCullTileconeMV>(a, b, e, tile_id)
-                          : tile_class<VB_CULL_TILECONE>(a, b, e, tile_id);
-  if (a.cull == VB_CULL_EXACT) return tile_class<VB_CULL_EXACT>(a, b, e, tile_id);
-  return tile_class<VB_CULL_NONE>(a, b, e, tile_id);
+    return a.mask_visible ? tile_class<kCullTileconeMV>(a, b, tile_id) : tile_class<VB_CULL_TILECONE>(a, b, tile_id);
+  if (a.cull == VB_CULL_EXACT) return tile_class<VB_CULL_EXACT>(a, b, tile_id);
+  return tile_class<VB_CULL_NONE>(a, b, tile_id);
 }
 
-// Loads half-baseline ih (upstream: viss_recon_kernel.cuh:231-240,
-// ..._vissfast.cuh:476-497): its phase data into b, its endpoint data into e.
-__device__ __forceinline__ void load_baseline(const S1Args& a, int ih, bool raw, BPhase& b, Ends& e) {
+// Loads half-baseline ih into registers (upstream: viss_recon_kernel.cuh:231-240,
+// ..._vissfast.cuh:476-497).
+__device__ __forceinline__ void load_baseline(const S1Args& a, int ih, bool raw, Baseline& b) {
   b.active = ih < a.n_half;
   const int i = b.active ? half_to_full_pos(ih, a.nbl) : 0;
   float uu = b.active ? a.u[i] : 0.f, vv = b.active ? a.v[i] : 0.f, ww = b.active ? a.w[i] : 0.f;
@@ -202,14 +151,16 @@ __device__ __forceinline__ void load_baseline(const S1Args& a, int ih, bool raw,
   const float kk = -2.0f * 3.14159265358979323846f;
   b.ku = kk * uu; b.kv = kk * vv; b.kw = kk * ww;
   if (a.blockage && b.active) {
-    e.x1 = a.x1[i]; e.y1 = a.y1[i]; e.z1 = a.z1[i]; e.i1 = a.in1[i];
-    e.x2 = a.x2[i]; e.y2 = a.y2[i]; e.z2 = a.z2[i]; e.i2 = a.in2[i];
-    e.c1 = a.cp1 ? a.cp1[i] : a.cosphi;
-    e.c2 = a.cp2 ? a.cp2[i] : a.cosphi;
+    b.x1 = a.x1[i]; b.y1 = a.y1[i]; b.z1 = a.z1[i]; b.i1 = a.in1[i];
+    b.x2 = a.x2[i]; b.y2 = a.y2[i]; b.z2 = a.z2[i]; b.i2 = a.in2[i];
+    b.c1 = a.cp1 ? a.cp1[i] : a.cosphi;
+    b.c2 = a.cp2 ? a.cp2[i] : a.cosphi;
   } else {
-    e.x1 = e.y1 = e.z1 = e.i1 = e.x2 = e.y2 = e.z2 = e.i2 = 0.f;
-    e.c1 = e.c2 = a.cosphi;
+    b.x1 = b.y1 = b.z1 = b.i1 = b.x2 = b.y2 = b.z2 = b.i2 = 0.f;
+    b.c1 = b.c2 = a.cosphi;
   }
+  b.ux1 = b.x1 * b.i1; b.uy1 = b.y1 * b.i1; b.uz1 = b.z1 * b.i1;
+  b.ux2 = b.x2 * b.i2; b.uy2 = b.y2 * b.i2; b.uz2 = b.z2 * b.i2;
   b.cls = b.tcls = kClsHid;
 }
 
@@ -224,7 +175,7 @@ __device__ constexpr bool pixel_dither() {
 }
 
 template <int MODE, int PAR>
-__device__ __forceinline__ void phase_sincos(const BPhase& b, const double2 lm, const double nd,
+__device__ __forceinline__ void phase_sincos(const Baseline& b, const double2 lm, const double nd,
                                              const float4 f, const float nm1, float& s, float& c,
                                              double& sd, double& cd, bool raw) {
   if constexpr (MODE == VB_PREC_FP32_FP64PH) {
@@ -264,43 +215,11 @@ __device__ __forceinline__ void phase_sincos(const BPhase& b, const double2 lm, 
   }
 }
 
-// FP64-phase modes (F32X, FP64) split in two: the ring part of the phase, w n
-// (+ the F32X magic constant, or - w for the uncorrected phase), formed once
-// per pixel pair whose pixels share n, and the rest, u l + v m, per pixel.
-// The operations and their order are those of phase_sincos.
-template <int MODE>
-__device__ __forceinline__ double phase_ring(const BPhase& b, const double nd, bool raw) {
-  if constexpr (MODE == VB_PREC_FP32_FP64PH) return fma(b.W, nd, b.C);
-  else return b.W * (raw ? (nd - 1.0) : nd);
-}
-template <int MODE, int PAR>
-__device__ __forceinline__ void sincos_ring(const BPhase& b, const double2 lm, const double T, float& s, float& c,
-                                            double& sd, double& cd) {
-  const double t = fma(b.U, lm.x, fma(b.V, lm.y, T));
-  if constexpr (MODE == VB_PREC_FP32_FP64PH) {
-    const unsigned lo = (unsigned)__double2loint(t);
-    const unsigned kb = (lo & 0x7FFFFFu) ^ (PAR ? 0x4B400000u : 0x4B000000u);
-    float ang = __fmaf_rn(__uint_as_float(kb), kAngScale, -kTwoPiF);
-    __sincosf(ang, &s, &c);
-  } else {
-    sincos(-6.283185307179586476925286766559 * t, &sd, &cd);
-  }
-}
-
 // Imaginary-part sign of the accumulated sums: F32X/DS accumulate sin(+2 pi t).
 template <int MODE>
 __device__ constexpr float imag_sign() {
   return (MODE == VB_PREC_FP32_FP64PH || MODE == VB_PREC_FP32_DSPH) ? -1.0f : 1.0f;
 }
-
-// Dynamic shared memory of one CTA: the staged pixel pairs and FP32 records,
-// then the endpoint data of every thread's baselines.
-__host__ __device__ constexpr size_t s1_smem_bytes(int stage_pix, int bpt) {
-  return (size_t)(stage_pix / 2) * sizeof(PixPair) + (size_t)stage_pix * sizeof(float4) +
-         (bpt > 2 ? (size_t)bpt * kEndFields * S1_THREADS * sizeof(float) : 0);
-}
-// smallest pairing block: 32 pixels (the smallest stage / tile / sub-tile)
-constexpr int kStageBlocksMax = 2048 / 32;
 
 // Register budget per thread: 80 for 3 resident CTAs of 256 threads; 120 for
 // 2 (measured: 120 beats the full 128 the 2-CTA budget allows by ~2 % on the
@@ -308,22 +227,14 @@ constexpr int kStageBlocksMax = 2048 / 32;
 template <int MODE, int BPT, int MINB, int CULL>
 __global__ void __maxnreg__(MINB == 3 ? 80 : 120) k_stage1(const S1Args a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  PixPair* s_pair = reinterpret_cast<PixPair*>(smem_raw);
-  float4* s_f4 = reinterpret_cast<float4*>(smem_raw + (size_t)(a.stage_pix / 2) * sizeof(PixPair));
-  float* s_ep = reinterpret_cast<float*>(smem_raw + (size_t)(a.stage_pix / 2) * sizeof(PixPair) +
-                                         (size_t)a.stage_pix * sizeof(float4));
+  PixRec* s_px = reinterpret_cast<PixRec*>(smem_raw);
   __shared__ int s_item;
-  __shared__ int s_shared[kStageBlocksMax];
   __shared__ unsigned long long s_cnt[4];
 
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
   const bool raw = (a.phase_corrected == 0);
   constexpr bool kDoubleAcc = (MODE == VB_PREC_FP64);
-  // FP64-phase modes share the ring part of the phase within a pixel pair
-  constexpr bool kRing = (MODE == VB_PREC_FP32_FP64PH || MODE == VB_PREC_FP64);
-  constexpr bool kEndsInRegs = (BPT <= 2);
-  const int bp = a.pair_blk;
 
   if (threadIdx.x < 4) s_cnt[threadIdx.x] = 0ull;
 
@@ -338,18 +249,13 @@ __global__ void __maxnreg__(MINB == 3 ? 80 : 120) k_stage1(const S1Args a) {
     const int chunk = item / a.n_btile;
     const int btile = item - chunk * a.n_btile;
 
-    // --- per-thread baselines: phase data in registers; endpoint data in
-    // registers too with up to 2 baselines per thread, in shared memory with 4
-    BPhase bl[BPT];
-    Ends er[kEndsInRegs ? BPT : 1];
+    // --- per-thread baselines -------------------------------------------------
+    Baseline bl[BPT];
 #pragma unroll
     for (int k = 0; k < BPT; ++k) {
-      BPhase& b = bl[k];
+      Baseline& b = bl[k];
       const int ih = btile * (S1_THREADS * BPT) + warp * (32 * BPT) + k * 32 + lane;
-      Ends e;
-      load_baseline(a, ih, raw, b, e);
-      if constexpr (kEndsInRegs) er[k] = e;
-      else store_ends(s_ep, k, e);
+      load_baseline(a, ih, raw, b);
       const float uu = b.uf, vv = b.vf, ww = b.wf;
       if (MODE == VB_PREC_FP32_FP64PH && b.active &&
           (fabsf(uu) >= (float)kMaxUvwF32X || fabsf(vv) >= (float)kMaxUvwF32X ||
@@ -357,32 +263,19 @@ __global__ void __maxnreg__(MINB == 3 ? 80 : 120) k_stage1(const S1Args a) {
         atomicOr(a.err, ERR_PHASE_RANGE);
     }
 
-    // endpoint data of baseline k, wherever it is kept
-    auto ends = [&](const int k) -> Ends {
-      if constexpr (kEndsInRegs) return er[k];
-      else return load_ends(s_ep, k);
-    };
-
     double accR[BPT], accI[BPT];
     float kcR[BPT], kcI[BPT];   // Kahan compensation (DS)
 #pragma unroll
     for (int k = 0; k < BPT; ++k) { accR[k] = 0.0; accI[k] = 0.0; kcR[k] = 0.f; kcI[k] = 0.f; }
 
-    // term counters: warp-uniform values, added per tile by lane 0 into the
-    // CTA's shared counters (no registers held across the pixel loops); the
-    // pad pixels past npix are not counted
-    int nact_g = 0;
+    unsigned long long cnt_fast = 0, cnt_mask = 0, cnt_hid = 0, cnt_all = 0;
+    int nact = 0;
 #pragma unroll
-    for (int k = 0; k < BPT; ++k) nact_g += __popc(__ballot_sync(0xffffffffu, bl[k].active));
-    auto count = [&](int which, int64_t q0, int64_t q1) {
-      if (q1 > a.npix) q1 = a.npix;
-      if (a.counters && lane == 0 && q1 > q0) atomicAdd(&s_cnt[which], (unsigned long long)nact_g * (q1 - q0));
-    };
+    for (int k = 0; k < BPT; ++k) nact += __popc(__ballot_sync(0xffffffffu, bl[k].active));
 
-    // pixel ranges cover whole pairing blocks (pad pixels have B = 0)
     const int64_t p_begin = (int64_t)chunk * a.chunk_pix;
     int64_t p_end = p_begin + a.chunk_pix;
-    if (p_end > a.npix_pad) p_end = a.npix_pad;
+    if (p_end > a.npix) p_end = a.npix;
 
     for (int64_t t0 = p_begin; t0 < p_end; t0 += a.cull_tile) {
       int64_t t1 = t0 + a.cull_tile;
@@ -393,8 +286,8 @@ __global__ void __maxnreg__(MINB == 3 ? 80 : 120) k_stage1(const S1Args a) {
       bool any_live = false, any_mix = false;
 #pragma unroll
       for (int k = 0; k < BPT; ++k) {
-        BPhase& b = bl[k];
-        const int cls = tile_class<CULL>(a, b, ends(k), tile_id);
+        Baseline& b = bl[k];
+        const int cls = tile_class<CULL>(a, b, tile_id);
         b.cls = b.tcls = cls;
         any_live |= (cls != kClsHid);
         any_mix |= (cls == kClsMix);
@@ -403,29 +296,28 @@ __global__ void __maxnreg__(MINB == 3 ? 80 : 120) k_stage1(const S1Args a) {
       const bool warp_mix = __any_sync(0xffffffffu, any_mix);
       // mixed tiles refined into exact sub-tiles count their terms per sub-tile
       const bool refine = is_tilecone<CULL>() && warp_mix && a.refine_pix > 0;
-      count(3, t0, t1);
-      if (!warp_live) count(2, t0, t1);
-      else if (!warp_mix) count(0, t0, t1);
-      else if (!refine) count(1, t0, t1);
+      const int64_t tile_terms = (int64_t)nact * (t1 - t0);
+      cnt_all += tile_terms;
+      if (!warp_live) cnt_hid += tile_terms;
+      else if (!warp_mix) cnt_fast += tile_terms;
+      else if (!refine) cnt_mask += tile_terms;
 
       if (!__syncthreads_or(warp_live ? 1 : 0)) continue;
 
       for (int64_t s0 = t0; s0 < t1; s0 += a.stage_pix) {
         const int ns = (int)((t1 - s0) < a.stage_pix ? (t1 - s0) : a.stage_pix);
         __syncthreads();
-        {
-          const float4* gp = reinterpret_cast<const float4*>(a.pairs + s0 / 2);
-          float4* sp = reinterpret_cast<float4*>(s_pair);
-          const int nq = ns * (int)(sizeof(PixPair) / sizeof(float4)) / 2;
-          for (int j = threadIdx.x; j < nq; j += S1_THREADS) sp[j] = gp[j];
-          for (int j = threadIdx.x; j < ns; j += S1_THREADS) s_f4[j] = a.f4[s0 + j];
-          const int nb = ns / bp;
-          for (int j = threadIdx.x; j < nb; j += S1_THREADS) s_shared[j] = a.pair_shared[s0 / bp + j];
+        for (int j = threadIdx.x; j < ns; j += S1_THREADS) {
+          PixRec r;
+          r.lm = a.lm[s0 + j];
+          r.nb = a.nb[s0 + j];
+          r.f4 = a.f4[s0 + j];
+          s_px[j] = r;
         }
         __syncthreads();
         if (!warp_live) continue;
 
-        // two interleaved FP32 partial sums per baseline (even / odd slots)
+        // two interleaved FP32 partial sums per baseline (even / odd pixels)
         float pR0[BPT], pI0[BPT], pR1[BPT], pI1[BPT];
         double dR[BPT], dI[BPT];
 #pragma unroll
@@ -434,154 +326,65 @@ __global__ void __maxnreg__(MINB == 3 ? 80 : 120) k_stage1(const S1Args a) {
           dR[k] = dI[k] = 0.0;
         }
 
-        // accumulates one term of baseline k into the even (SLOT 0) or odd
-        // (SLOT 1) sums with weight Bw (B, or 0 where the term is excluded)
-        auto acc = [&](const int k, const float Bw, const float sn, const float cs, const double sd,
-                       const double cd, auto slot_tag) {
-          if constexpr (kDoubleAcc) {
-            dR[k] = fma((double)Bw, cd, dR[k]);
-            dI[k] = fma((double)Bw, sd, dI[k]);
-          } else if constexpr (decltype(slot_tag)::value == 1) {
-            pR1[k] = fmaf(Bw, cs, pR1[k]);
-            pI1[k] = fmaf(Bw, sn, pI1[k]);
-          } else {
-            pR0[k] = fmaf(Bw, cs, pR0[k]);
-            pI0[k] = fmaf(Bw, sn, pI0[k]);
-          }
-        };
-        using S0 = std::integral_constant<int, 0>;
-        using S1 = std::integral_constant<int, 1>;
-        // odd slots take the half-turn dither in the modes that use it
-        constexpr int kOddPar = pixel_dither<MODE>() ? 1 : 0;
-
-        // staged pair q (slots 2q, 2q + 1) for every baseline of the thread.
-        // PATH 0: every baseline of the warp is included; 1: each baseline by
-        // its class (visible or hidden, no per-pixel test).  SHARED: both
-        // pixels lie on one ring (same n).
-        auto pair_all = [&](const int q, auto path_tag, auto shared_tag) {
+        // one pixel.  PATH 0: every baseline of the warp is included; 1: each
+        // baseline by its class (visible or hidden, no per-pixel test); 2: the
+        // per-pixel occlusion test for mixed baselines (visible ones included
+        // unconditionally, hidden excluded)
+        auto pixel = [&](const int j, float (&aR)[BPT], float (&aI)[BPT], auto path_tag, auto par_tag) {
           constexpr int PATH = decltype(path_tag)::value;
-          if constexpr (kRing) {
-            constexpr bool SHARED = decltype(shared_tag)::value != 0;
-            const PixPair* pr = s_pair + q;
-            const double2 lm0 = pr->lm0, lm1 = pr->lm1;
-            const float4 w3 = *reinterpret_cast<const float4*>(&pr->n0);
-            const double n0 = __hiloint2double(__float_as_int(w3.y), __float_as_int(w3.x));
-            double n1 = n0;
-            if constexpr (!SHARED) {
-              const float4 w4 = *reinterpret_cast<const float4*>(&pr->n1);
-              n1 = __hiloint2double(__float_as_int(w4.y), __float_as_int(w4.x));
-            }
+          constexpr bool MASKED = (PATH == 2);
+          constexpr int PAR = decltype(par_tag)::value;
+          const PixRec* rp = s_px + j;
+          const double2 lm = rp->lm;
+          const float4 nb = rp->nb;
+          const double nd = __hiloint2double(__float_as_int(nb.y), __float_as_int(nb.x));
+          float4 f;
+          if constexpr (MASKED || MODE == VB_PREC_FP32_DSPH || MODE == VB_PREC_REF32) f = rp->f4;
+          else f = make_float4(0.f, 0.f, 0.f, nb.z);
+          const float Bp = nb.z;
 #pragma unroll
-            for (int k = 0; k < BPT; ++k) {
-              float B0 = w3.z, B1 = w3.w;
-              if constexpr (PATH == 1) {
-                const bool inc = bl[k].cls != kClsHid;
-                B0 = inc ? B0 : 0.0f;
-                B1 = inc ? B1 : 0.0f;
-              }
-              const double T0 = phase_ring<MODE>(bl[k], n0, raw);
-              const double T1 = SHARED ? T0 : phase_ring<MODE>(bl[k], n1, raw);
-              float s0, c0, s1, c1;
-              double sd0, cd0, sd1, cd1;
-              sincos_ring<MODE, 0>(bl[k], lm0, T0, s0, c0, sd0, cd0);
-              sincos_ring<MODE, kOddPar>(bl[k], lm1, T1, s1, c1, sd1, cd1);
-              acc(k, B0, s0, c0, sd0, cd0, S0{});
-              acc(k, B1, s1, c1, sd1, cd1, S1{});
+          for (int k = 0; k < BPT; ++k) {
+            const Baseline& b = bl[k];
+            bool inc = true;
+            if constexpr (MASKED) {
+              const float o1 = occ_dot(f.x, f.y, f.z, b.x1, b.y1, b.z1, b.i1);
+              const float o2 = occ_dot(f.x, f.y, f.z, b.x2, b.y2, b.z2, b.i2);
+              const bool pass = !(o1 < b.c1 || o2 < b.c2);
+              inc = (b.cls == kClsVis) || (b.cls == kClsMix && pass);
+            } else if constexpr (PATH == 1) {
+              inc = (b.cls != kClsHid);
             }
-          } else {
-            const float4 f0 = s_f4[2 * q], f1 = s_f4[2 * q + 1];
-            const double2 dz = make_double2(0.0, 0.0);
-#pragma unroll
-            for (int k = 0; k < BPT; ++k) {
-              float B0 = f0.w, B1 = f1.w;
-              if constexpr (PATH == 1) {
-                const bool inc = bl[k].cls != kClsHid;
-                B0 = inc ? B0 : 0.0f;
-                B1 = inc ? B1 : 0.0f;
-              }
-              float s0, c0, s1, c1;
-              double sd0, cd0, sd1, cd1;
-              phase_sincos<MODE, 0>(bl[k], dz, 0.0, f0, f0.z - 1.0f, s0, c0, sd0, cd0, raw);
-              phase_sincos<MODE, kOddPar>(bl[k], dz, 0.0, f1, f1.z - 1.0f, s1, c1, sd1, cd1, raw);
-              acc(k, B0, s0, c0, sd0, cd0, S0{});
-              acc(k, B1, s1, c1, sd1, cd1, S1{});
+            float sn, cs;
+            double sd, cd;
+            phase_sincos<MODE, PAR>(b, lm, nd, f, nb.w, sn, cs, sd, cd, raw);
+            if constexpr (kDoubleAcc) {
+              const double Bw = inc ? (double)Bp : 0.0;
+              dR[k] = fma(Bw, cd, dR[k]);
+              dI[k] = fma(Bw, sd, dI[k]);
+            } else {
+              const float Bw = inc ? Bp : 0.0f;
+              aR[k] = fmaf(Bw, cs, aR[k]);
+              aI[k] = fmaf(Bw, sn, aI[k]);
             }
           }
-        };
-        // staged pair q for baseline k with the per-pixel occlusion test (mixed
-        // baselines; visible ones included unconditionally, hidden excluded)
-        auto pair_masked = [&](const int q, const int k, const Ends& e) {
-          const float4 f0 = s_f4[2 * q], f1 = s_f4[2 * q + 1];
-          const int cls = bl[k].cls;
-          const bool p0 = !(occ_dot(f0.x, f0.y, f0.z, e.x1, e.y1, e.z1, e.i1) < e.c1 ||
-                            occ_dot(f0.x, f0.y, f0.z, e.x2, e.y2, e.z2, e.i2) < e.c2);
-          const bool p1 = !(occ_dot(f1.x, f1.y, f1.z, e.x1, e.y1, e.z1, e.i1) < e.c1 ||
-                            occ_dot(f1.x, f1.y, f1.z, e.x2, e.y2, e.z2, e.i2) < e.c2);
-          const float B0 = ((cls == kClsVis) || (cls == kClsMix && p0)) ? f0.w : 0.0f;
-          const float B1 = ((cls == kClsVis) || (cls == kClsMix && p1)) ? f1.w : 0.0f;
-          float s0, c0, s1, c1;
-          double sd0, cd0, sd1, cd1;
-          if constexpr (kRing) {
-            const PixPair* pr = s_pair + q;
-            const double2 lm0 = pr->lm0, lm1 = pr->lm1;
-            const float4 w3 = *reinterpret_cast<const float4*>(&pr->n0);
-            const float4 w4 = *reinterpret_cast<const float4*>(&pr->n1);
-            const double n0 = __hiloint2double(__float_as_int(w3.y), __float_as_int(w3.x));
-            const double n1 = __hiloint2double(__float_as_int(w4.y), __float_as_int(w4.x));
-            sincos_ring<MODE, 0>(bl[k], lm0, phase_ring<MODE>(bl[k], n0, raw), s0, c0, sd0, cd0);
-            sincos_ring<MODE, kOddPar>(bl[k], lm1, phase_ring<MODE>(bl[k], n1, raw), s1, c1, sd1, cd1);
-          } else {
-            const double2 dz = make_double2(0.0, 0.0);
-            phase_sincos<MODE, 0>(bl[k], dz, 0.0, f0, f0.z - 1.0f, s0, c0, sd0, cd0, raw);
-            phase_sincos<MODE, kOddPar>(bl[k], dz, 0.0, f1, f1.z - 1.0f, s1, c1, sd1, cd1, raw);
-          }
-          acc(k, B0, s0, c0, sd0, cd0, S0{});
-          acc(k, B1, s1, c1, sd1, cd1, S1{});
         };
         using Unmasked = std::integral_constant<int, 0>;
         using Select = std::integral_constant<int, 1>;
-        using Shared = std::integral_constant<int, 1>;
-        using Own = std::integral_constant<int, 0>;
+        using Masked = std::integral_constant<int, 2>;
+        using Even = std::integral_constant<int, 0>;
+        using Odd = std::integral_constant<int, pixel_dither<MODE>() ? 1 : 0>;
 
-        // slots [j0, j1) of the staged block (whole pairing blocks): per block
-        // its ring pairs, then its other pairs
+        // pixels [j0, j1) of the staged tile (j0 even: pixel parity = index parity)
         auto run = [&](const int j0, const int j1, auto path_tag) {
-          for (int b0 = j0; b0 < j1; b0 += bp) {
-            const int q0 = b0 >> 1, qe = q0 + (bp >> 1);
-            const int qs = kRing ? q0 + s_shared[b0 / bp] : q0;
-            // with 2 baselines per thread two pairs per trip keep enough chains
-            // in flight; with 4, one
-            if constexpr (BPT >= 4) {
-#pragma unroll 1
-              for (int q = q0; q < qs; ++q) pair_all(q, path_tag, Shared{});
-            } else {
+          int j = j0;
+          // two pixel pairs per trip: 0.5 % faster than the compiler's choice
+          // (no unroll 1: +5 %, unroll 3 / 4: +5-6 %)
 #pragma unroll 2
-              for (int q = q0; q < qs; ++q) pair_all(q, path_tag, Shared{});
-            }
-            for (int q = qs; q < qe; ++q) pair_all(q, path_tag, Own{});
+          for (; j + 1 < j1; j += 2) {
+            pixel(j, pR0, pI0, path_tag, Even{});
+            pixel(j + 1, pR1, pI1, path_tag, Odd{});
           }
-        };
-        // the per-pixel test, one baseline at a time: its endpoint data comes
-        // into registers once for the whole range; a baseline that no lane of
-        // the warp needs is skipped
-        auto run_masked = [&](const int j0, const int j1) {
-          if constexpr (kEndsInRegs) {
-            // every baseline of the thread per pair: the pair's records are
-            // read once for all of them
-#pragma unroll 2
-            for (int q = j0 >> 1; q < (j1 >> 1); ++q) {
-#pragma unroll
-              for (int k = 0; k < BPT; ++k) pair_masked(q, k, er[k]);
-            }
-          } else {
-#pragma unroll
-            for (int k = 0; k < BPT; ++k) {
-              if (!__any_sync(0xffffffffu, bl[k].cls != kClsHid)) continue;
-              const Ends e = load_ends(s_ep, k);
-#pragma unroll 2
-              for (int q = j0 >> 1; q < (j1 >> 1); ++q) pair_masked(q, k, e);
-            }
-          }
+          if (j < j1) pixel(j, pR0, pI0, path_tag, Even{});
         };
 
         if (!warp_mix) {
@@ -597,9 +400,10 @@ __global__ void __maxnreg__(MINB == 3 ? 80 : 120) k_stage1(const S1Args a) {
             bool l_live = false, l_mix = false, l_newhid = false;
 #pragma unroll
             for (int k = 0; k < BPT; ++k) {
-              BPhase& b = bl[k];
+              Baseline& b = bl[k];
               int e = b.tcls;
-              if (e == kClsMix) e = exact_tile_class(a.subcones + sub_id, ends(k));
+              if (e == kClsMix)
+                e = exact_tile_class(a.subcones + sub_id, b.x1, b.y1, b.z1, b.i1, b.c1, b.x2, b.y2, b.z2, b.i2, b.c2);
               b.cls = e;
               l_live |= (e != kClsHid);
               l_mix |= (e == kClsMix);
@@ -608,18 +412,19 @@ __global__ void __maxnreg__(MINB == 3 ? 80 : 120) k_stage1(const S1Args a) {
             const bool w_live = __any_sync(0xffffffffu, l_live);
             const bool w_mix = __any_sync(0xffffffffu, l_mix);
             const bool w_newhid = __any_sync(0xffffffffu, l_newhid);
-            if (!w_live) count(2, s0 + r0, s0 + r1);
-            else if (w_mix) count(1, s0 + r0, s0 + r1);
-            else count(0, s0 + r0, s0 + r1);
+            const int64_t sub_terms = (int64_t)nact * (r1 - r0);
+            if (!w_live) cnt_hid += sub_terms;
+            else if (w_mix) cnt_mask += sub_terms;
+            else cnt_fast += sub_terms;
             if (!w_live) continue;
-            if (w_mix) run_masked(r0, r1);
+            if (w_mix) run(r0, r1, Masked{});
             else if (w_newhid) run(r0, r1, Select{});
             else run(r0, r1, Unmasked{});
           }
         } else {
-          run_masked(0, ns);
+          run(0, ns, Masked{});
         }
-        // the odd-slot sums were taken half a turn on: subtract them
+        // the odd-pixel sums were taken half a turn on: subtract them
         constexpr float kOddSign = pixel_dither<MODE>() ? -1.0f : 1.0f;
 
         // fold the staged-tile partials into the running totals
@@ -657,99 +462,15 @@ __global__ void __maxnreg__(MINB == 3 ? 80 : 120) k_stage1(const S1Args a) {
         a.partial[(int64_t)chunk * a.n_half + ih] =
             make_double2(accR[k], (double)imag_sign<MODE>() * accI[k]);
     }
+    if (a.counters && lane == 0) {
+      atomicAdd(&s_cnt[0], cnt_fast);
+      atomicAdd(&s_cnt[1], cnt_mask);
+      atomicAdd(&s_cnt[2], cnt_hid);
+      atomicAdd(&s_cnt[3], cnt_all);
+    }
   }
   __syncthreads();
   if (a.counters && threadIdx.x < 4) atomicAdd(&a.counters[threadIdx.x], s_cnt[threadIdx.x]);
-}
-
-// Packs the sky into pair records and FP32 records, block by block in pairing
-// order (the order table is the same for every block); ring pairs whose two n
-// differ in any bit (a sky that is not HEALPix) are demoted to the block's
-// other pairs.  One CTA of kPairBlkMax threads per block.
-__global__ void __launch_bounds__(kPairBlkMax) k_pack_pairs(const float* __restrict__ B, const float* __restrict__ l,
-                                                          const float* __restrict__ m, const float* __restrict__ n,
-                                                          int64_t npix, int64_t nblk, const PairOrder ord,
-                                                          PixPair* __restrict__ pairs, float4* __restrict__ f4,
-                                                          int* __restrict__ pair_shared) {
-  __shared__ float s_l[kPairBlkMax], s_m[kPairBlkMax], s_n[kPairBlkMax], s_B[kPairBlkMax];
-  __shared__ short s_ord[kPairBlkMax];
-  const int bp = ord.bp;
-  const int t = threadIdx.x;
-  for (int64_t blk = blockIdx.x; blk < nblk; blk += gridDim.x) {
-    const int64_t base = blk * bp;
-    __syncthreads();
-    if (t < bp) {
-      const int64_t i = base + t;
-      const bool real = i < npix;
-      s_l[t] = real ? l[i] : 0.f;
-      s_m[t] = real ? m[i] : 0.f;
-      s_n[t] = real ? n[i] : 0.f;
-      s_B[t] = real ? B[i] : 0.f;
-    }
-    __syncthreads();
-    if (t == 0) {
-      // ring pairs that hold (bitwise equal n first, in order), then the
-      // demoted ones, then the leftover pairs
-      int w = 0;
-      for (int q = 0; q < ord.shared; ++q) {
-        const int a0 = ord.src[2 * q], a1 = ord.src[2 * q + 1];
-        if (__float_as_uint(s_n[a0]) == __float_as_uint(s_n[a1])) { s_ord[w++] = (short)a0; s_ord[w++] = (short)a1; }
-      }
-      const int ok = w / 2;
-      for (int q = 0; q < ord.shared; ++q) {
-        const int a0 = ord.src[2 * q], a1 = ord.src[2 * q + 1];
-        if (__float_as_uint(s_n[a0]) != __float_as_uint(s_n[a1])) { s_ord[w++] = (short)a0; s_ord[w++] = (short)a1; }
-      }
-      for (int j = 2 * ord.shared; j < bp; ++j) s_ord[w++] = ord.src[j];
-      pair_shared[blk] = ok;
-    }
-    __syncthreads();
-    if (t < bp) {
-      const int src = s_ord[t];
-      f4[base + t] = make_float4(s_l[src], s_m[src], s_n[src], s_B[src]);
-      if ((t & 1) == 0) {
-        const int o = s_ord[t + 1];
-        PixPair pr;
-        pr.lm0 = make_double2((double)s_l[src], (double)s_m[src]);
-        pr.lm1 = make_double2((double)s_l[o], (double)s_m[o]);
-        pr.n0 = (double)s_n[src];
-        pr.B0 = s_B[src];
-        pr.B1 = s_B[o];
-        pr.n1 = (double)s_n[o];
-        pr.pad0 = pr.pad1 = 0.f;
-        pairs[(base + t) / 2] = pr;
-      }
-    }
-  }
-}
-
-// Pairing order of a block of bp NEST pixels (see PairOrder), from the face
-// coordinates of the local index: x = its even bits, y = its odd bits; the
-// ring is x + y (HEALPix ring index = face row * nside - (x + y) - 1).
-static PairOrder pair_order(int bp) {
-  PairOrder o{};
-  o.bp = bp;
-  std::vector<std::vector<int>> rings;
-  for (int i = 0; i < bp; ++i) {
-    int x = 0, y = 0;
-    for (int bit = 0; (1 << (2 * bit)) < bp; ++bit) {
-      x |= ((i >> (2 * bit)) & 1) << bit;
-      y |= ((i >> (2 * bit + 1)) & 1) << bit;
-    }
-    const size_t r = (size_t)(x + y);
-    if (rings.size() <= r) rings.resize(r + 1);
-    rings[r].push_back(i);
-  }
-  int w = 0;
-  std::vector<int> left;
-  for (auto& r : rings) {
-    size_t k = 0;
-    for (; k + 1 < r.size(); k += 2) { o.src[w++] = (short)r[k]; o.src[w++] = (short)r[k + 1]; }
-    if (k < r.size()) left.push_back(r[k]);
-  }
-  o.shared = w / 2;
-  for (int i : left) o.src[w++] = (short)i;
-  return o;
 }
 
 // V[ih] = sum over chunks of the partials, in chunk order (accumulate: V += that sum).
@@ -892,20 +613,9 @@ int stage1_plan(const vb_sky* sky, const vb_baselines* bl, const vb_stage1_opts*
     if (r < q.cull_tile && r <= q.stage_pix) q.refine_pix = r;
   }
 
-  // ring-pairing block: divides every range the kernel walks (stages, cull
-  // tiles, refinement sub-tiles), at most 128 pixels; the packed sky is padded
-  // to a whole block with pixels of brightness 0
-  int pb = kPairBlkMax;
-  pb = std::min(pb, q.cull_tile);
-  pb = std::min(pb, q.stage_pix);
-  if (q.refine_pix > 0) pb = std::min(pb, q.refine_pix);
-  if (pb < 2 || q.stage_pix / pb > kStageBlocksMax)
-    return fail(VB_ERR_INVALID, "stage 1: cull tile %d too small (at least 32 pixels)", q.cull_tile);
-  q.pair_blk = pb;
-  q.npix_pad = ceil_div(q.npix, pb) * pb;
   const int per_tile = S1_THREADS * q.bpt;
   q.n_btile = (int)ceil_div(q.n_half, per_tile);
-  size_t smem = s1_smem_bytes(stage, q.bpt);
+  size_t smem = (size_t)stage * 48;
   int occ = occupancy(q.precision, q.bpt, q.minb, q.mask_visible ? kCullTileconeMV : q.cull, smem);
   int capacity = sm_count() * occ;
   q.grid = capacity;
@@ -938,9 +648,9 @@ size_t stage1_carve(const Stage1Plan& p, void* ws, size_t cap, Stage1Buffers* b,
   Stage1Buffers x;
   x.err = c.take<unsigned>(4);   // first: vb_workspace_error_flags reads it at offset 0
   if (pack_pixels) {
-    x.pairs = c.take<PixPair>((size_t)(p.npix_pad / 2));
-    x.f4 = c.take<float4>((size_t)p.npix_pad);
-    x.pair_shared = c.take<int>((size_t)(p.npix_pad / p.pair_blk));
+    x.lm = c.take<double2>(p.npix);
+    x.nb = c.take<float4>(p.npix);
+    x.f4 = c.take<float4>(p.npix);
     if (p.cull == VB_CULL_EXACT) x.cones = c.take<ExactCone>(p.ntile_cull);
     if (p.refine_pix > 0) x.subcones = c.take<ExactCone>((size_t)ceil_div(p.npix, p.refine_pix));
   }
@@ -952,11 +662,7 @@ size_t stage1_carve(const Stage1Plan& p, void* ws, size_t cap, Stage1Buffers* b,
 }
 
 int stage1_prepare_pixels(const vb_sky* sky, const Stage1Plan& p, const Stage1Buffers& b, cudaStream_t s) {
-  const int64_t nblk = p.npix_pad / p.pair_blk;
-  const int grid = (int)std::min<int64_t>(nblk, (int64_t)sm_count() * 16);
-  k_pack_pairs<<<grid, kPairBlkMax, 0, s>>>(sky->B, sky->l, sky->m, sky->n, p.npix, nblk, pair_order(p.pair_blk),
-                                            b.pairs, b.f4, b.pair_shared);
-  VB_LAUNCH_CHECK();
+  VB_TRY(geom_pack_pixels(sky->B, sky->l, sky->m, sky->n, p.npix, b.lm, b.nb, b.f4, s));
   if (p.cull == VB_CULL_EXACT) VB_TRY(geom_exact_cones(p.cull_tile, sky->l, sky->m, sky->n, p.npix, b.cones, s));
   if (p.refine_pix > 0) VB_TRY(geom_exact_cones(p.refine_pix, sky->l, sky->m, sky->n, p.npix, b.subcones, s));
   return VB_OK;
@@ -968,8 +674,8 @@ int stage1_run(const vb_sky* sky, const vb_baselines* bl, const Stage1Plan& p, c
   if (p.n_half == 0) return VB_OK;
   if (!pixels_ready) VB_TRY(stage1_prepare_pixels(sky, p, b, s));
   S1Args a{};
-  a.pairs = b.pairs; a.f4 = b.f4; a.pair_shared = b.pair_shared;
-  a.npix = p.npix; a.npix_pad = p.npix_pad; a.pair_blk = p.pair_blk;
+  a.lm = b.lm; a.nb = b.nb; a.f4 = b.f4;
+  a.npix = p.npix;
   a.cull = p.cull; a.cull_tile = p.cull_tile; a.stage_pix = p.stage_pix; a.chunk_pix = p.chunk_pix;
   a.nchunk = p.nchunk; a.n_btile = p.n_btile; a.n_items = p.n_items;
   a.tcx = sky->cx; a.tcy = sky->cy; a.tcz = sky->cz; a.tcosA = sky->cosA; a.tsinA = sky->sinA;
@@ -984,7 +690,7 @@ int stage1_run(const vb_sky* sky, const vb_baselines* bl, const Stage1Plan& p, c
   a.n_half = p.n_half; a.nbl = p.nbl; a.blockage = p.blockage; a.phase_corrected = p.phase_corrected;
   a.queue = b.queue; a.partial = b.partial; a.counters = counters; a.err = b.err;
   VB_CUDA(cudaMemsetAsync(b.queue, 0, sizeof(int), s));
-  size_t smem = s1_smem_bytes(p.stage_pix, p.bpt);
+  size_t smem = (size_t)p.stage_pix * 48;
   const void* kern = stage1_kernel_of(p.precision, p.bpt, p.minb, p.mask_visible ? kCullTileconeMV : p.cull);
   VB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   void* args[] = {&a};
@@ -1055,10 +761,9 @@ __global__ void k_tile_classes(const S1Args a, int ntile, uint8_t* __restrict__ 
   for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < total; q += (int64_t)gridDim.x * blockDim.x) {
     const int ih = (int)(q / ntile);
     const int t = (int)(q - (int64_t)ih * ntile);
-    BPhase b;
-    Ends e;
-    load_baseline(a, ih, raw, b, e);
-    cls[q] = (uint8_t)tile_class_rt(a, b, e, t);
+    Baseline b;
+    load_baseline(a, ih, raw, b);
+    cls[q] = (uint8_t)tile_class_rt(a, b, t);
   }
 }
 }  // namespace vb
