@@ -172,6 +172,8 @@ int main(int argc, char** argv) {
   // 1: tiles the cone test proves visible skip the per-pixel test (the upstream
   // all-visible nm1 fast path); 0: they take it, only hidden tiles are culled
   int nm1_fast = to_int(get_arg(argc, argv, "--nm1_fast", "1"), 1);
+  // exact sub-tiles inside tile-cone mixed tiles: 0 = default (128 pixels), < 0 = off
+  int refine_pix = to_int(get_arg(argc, argv, "--refine_pix", "0"), 0);
   std::string prec_s = get_arg(argc, argv, "--precision", "fp32_fp64phase");
   std::string orbit_model = get_arg(argc, argv, "--orbit_model", "reference");
   int nsat = to_int(get_arg(argc, argv, "--nsat", "8"), 8);
@@ -292,6 +294,7 @@ int main(int argc, char** argv) {
   cfg.seg_seed = seg_seed;
   cfg.stage2_cull = stage2_cull;
   cfg.nm1_fast = nm1_fast ? 1 : 0;
+  cfg.stage1_refine_pix = refine_pix;
   cfg.slab_pix = slab_pix;
   cfg.use_graph = use_graph;
   cfg.device = 0;
