@@ -85,3 +85,60 @@ def test_faster_than_upstream_kernels(gpu, vb, ref, record_property):
     print(msg)
     record_property("speed", msg)
     assert ours1 < up1 and ours2 < up2, msg
+
+
+def test_stage1_at_the_production_launch_shape(gpu, vb, ref, record_property):
+    """One upstream production segment launch (10 MHz reference orbit, 6,981 time
+    steps = 195,468 half-baselines, tile-cone tiles of 256 pixels) on an
+    nside-256 sky: the upstream FP32 tile-cone kernel fills the GPU here, as
+    at the production size.  Both kernels are bound by the SFU (one sin and one
+    cos per evaluated term); the upstream evaluates every term of its
+    non-hidden tiles, which is this build's count with sub-tiles off (the tile
+    classes are bit-identical).  Reports both SFU fractions; fails if this
+    build is more than 10 % slower."""
+    from gpu_util import geometry, reference_baselines, tile_meta, sky_struct, bl_struct, stage1, upstream_cosphi
+    nside, tile = 256, 256
+    npix = 12 * nside * nside
+    (dl, dm, dn), _ = geometry(nside)
+    B = vb.synthetic_sky(nside, seed=1)
+    dB = dev((B.astype(np.float64) * (4 * np.pi / npix)).astype(np.float32))
+    host, d = reference_baselines(float(np.float32(30.0)), 1, 42, 0, 6981)
+    n_full = host["u"].size
+    nh = n_full // 2
+    meta = tile_meta(tile, dl, dm, dn, npix)
+    cp = upstream_cosphi()
+    sky = sky_struct(dl, dm, dn, dB, npix, (tile, meta))
+    bl = bl_struct(d, n_full, 28, cp)
+    sfu, f32, f64, clk = (C.c_double() for _ in range(4))
+    vb.check(vb.lib().vb_measure_peaks(C.byref(sfu), C.byref(f32), C.byref(f64), C.byref(clk)))
+    # evaluated terms: this build (sub-tiles on) and the upstream's (tile level)
+    _, cnt = stage1(sky, bl, precision=vb.PREC_FP32_FP64PH, cull=vb.CULL_TILECONE)
+    _, cnt_tile = stage1(sky, bl, precision=vb.PREC_FP32_FP64PH, cull=vb.CULL_TILECONE, refine_pix=-1)
+    ours_terms = int(cnt[0] + cnt[1])
+    up_terms = int(cnt_tile[3] - cnt_tile[2])
+    o = vb.Stage1Opts(precision=vb.PREC_FP32_FP64PH, cull=vb.CULL_TILECONE, phase_corrected=1, blockage=1)
+    need = vb.lib().vb_stage1_workspace_bytes(C.byref(sky), C.byref(bl), C.byref(o))
+    ws = zeros(need, np.uint8)
+    V = zeros(n_full, np.float64)
+
+    def ours():
+        vb.check(vb.lib().vb_viss_halfsym(C.byref(sky), C.byref(bl), C.byref(o), ws.ptr, need, V.ptr, None, None))
+        vb.check(vb.lib().vb_synchronize())
+    R = ref.ref_vf()
+    nm1 = zeros(npix)
+    vb.check(vb.lib().vb_build_nm1(dn.ptr, nm1.ptr, npix, None))
+    Vp = zeros(2 * nh)
+    args = [tile, vp(dB), vp(dl), vp(dm), vp(dn), vp(nm1), C.c_longlong(npix), *[vp(m) for m in meta], npix // tile,
+            *[vp(d[k]) for k in ("u", "v", "w", "x1", "y1", "z1", "invn1", "x2", "y2", "z2", "invn2")], nh,
+            C.c_float(cp), vp(Vp)]
+    t_up = _best(lambda: R.ref_vf_viss_tilecone(*args), 3)
+    t_ours = _best(ours, 3)
+    peak = sfu.value
+    f_up = up_terms / (t_up * 1e-3) / peak
+    f_ours = ours_terms / (t_ours * 1e-3) / peak
+    msg = (f"SPEED production launch shape (nside 256, {nh} half-baselines, tile 256): upstream FP32 {t_up:.2f} ms, "
+           f"{up_terms:.4g} evaluated terms, {f_up:.3f} of the SFU peak; this build {t_ours:.2f} ms, "
+           f"{ours_terms:.4g} terms, {f_ours:.3f} ({t_up / t_ours:.2f}x)")
+    print(msg)
+    record_property("speed_production_shape", msg)
+    assert t_ours <= 1.10 * t_up, msg
