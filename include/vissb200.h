@@ -297,7 +297,8 @@ typedef struct {
   int grid_res;         /* > 0 forces RES */
   float bl_max;         /* metres */
   float lambda;         /* metres */
-  int ppt;              /* pixels per thread of the occ_mode=2 / blockage=0 path: 1, 2 or 4 (0 = 2) */
+  int ppt;              /* pixels per thread of the occ_mode=2 / blockage=0 path: 1, 2 or 4
+                           (0 = 4 for VB_PREC_FP32_FP64PH, 2 otherwise) */
   int items_per_cta;    /* work-queue items (pixel block x group chunk) per resident CTA (0 = auto) */
 } vb_stage2_opts;
 

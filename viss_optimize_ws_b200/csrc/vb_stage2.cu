@@ -902,11 +902,14 @@ int stage2_plan(int n_half_total, int nseg, int64_t npix, const vb_stage2_opts* 
   q.cull = (o->cull == VB_CULL_EXACT && q.blockage && q.occ_mode == 2) ? VB_CULL_EXACT : VB_CULL_NONE;
   q.grid_res = o->grid_res;
   // pixels per thread of the representative / average path (the member path
-  // keeps one): 2 by default, 1, 2 or 4 on request
+  // keeps one): by default 4 with the FP64 phase in FP32 (its pair records are
+  // read once per 4 pixels; 0.835 against 0.772 of the SFU peak at nside 1024),
+  // 2 in the other modes (whose registers do not hold 4); 1, 2 or 4 on request
   if (o->ppt != 0 && o->ppt != 1 && o->ppt != 2 && o->ppt != 4)
     return fail(VB_ERR_INVALID, "stage 2: ppt=%d (0, 1, 2 or 4)", o->ppt);
   const bool members = q.blockage && q.occ_mode != 2;
-  q.ppt = members ? 1 : (o->ppt == 0 ? 2 : o->ppt);
+  const int ppt_auto = (o->precision == VB_PREC_FP32_FP64PH) ? 4 : 2;
+  q.ppt = members ? 1 : (o->ppt == 0 ? ppt_auto : o->ppt);
   q.bl_max = o->bl_max;
   q.lambda = o->lambda;
   q.n_half_total = n_half_total;
