@@ -14,7 +14,8 @@
  *    cudaStream_t passed as void* (NULL = legacy default stream).
  *  - The caller owns every buffer.  Kernel-level entry points never allocate;
  *    the ones that need scratch take a caller-provided workspace whose size a
- *    matching *_workspace_bytes() query returns.  Only the pipeline and orbit
+ *    matching *_workspace_bytes() query returns, at a 256-byte aligned address
+ *    (as cudaMalloc returns; VB_ERR_INVALID otherwise).  Only the pipeline and orbit
  *    objects (created once) allocate device memory, in their create calls.
  *  - Every call returns VB_OK (0) or a VB_ERR_* code and never exits the
  *    process; vb_last_error() gives a human-readable reason (thread-local).
@@ -48,7 +49,8 @@ extern "C" {
  * summed (the access behind VB_DEVERR_BAD_INDEX excepted, which is skipped), so
  * a non-zero word means the outputs of that call are not to be trusted.  The
  * host reads the word after the stream has finished. */
-#define VB_DEVERR_WAIT_TIMEOUT  1u  /* a bounded device-side wait gave up */
+#define VB_DEVERR_WAIT_TIMEOUT  1u  /* a bounded device-side wait gave up (stage 1: the bulk copy of
+                                       a stage of pixel records into shared memory did not land) */
 #define VB_DEVERR_BAD_INDEX     2u  /* an index check failed and the access was skipped */
 #define VB_DEVERR_HALFSYM       4u  /* the +/- pair layout of the baselines is violated */
 #define VB_DEVERR_PHASE_RANGE   8u  /* fp32_fp64phase: |u|+|v|+|w| of a term reached 2^28 turns, where

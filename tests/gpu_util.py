@@ -121,7 +121,9 @@ def tile_meta(tile_pix: int, dl, dm, dn, npix: int):
 
 
 def stage1(sky, bls, *, precision, cull, phase_corrected=1, blockage=1, bpt=0, stage_pix=0, chunk_pix=0,
-           exact_tile_pix=0, ctas_per_sm=0, items_per_cta=0, refine_pix=0):
+           exact_tile_pix=0, ctas_per_sm=0, items_per_cta=0, refine_pix=0, want_flags=False):
+    """vb_viss_halfsym on a fresh workspace: (V_half, term counters), plus the
+    workspace's device error word when want_flags is set."""
     o = vb.Stage1Opts(precision=precision, cull=cull, phase_corrected=phase_corrected, blockage=blockage, bpt=bpt,
                       stage_pix=stage_pix, chunk_pix=chunk_pix, exact_tile_pix=exact_tile_pix,
                       ctas_per_sm=ctas_per_sm, items_per_cta=items_per_cta, refine_pix=refine_pix)
@@ -133,6 +135,10 @@ def stage1(sky, bls, *, precision, cull, phase_corrected=1, blockage=1, bpt=0, s
     cnt = zeros(4, np.uint64)
     check(vb.lib().vb_viss_halfsym(C.byref(sky), C.byref(bls), C.byref(o), ws.ptr, need, V.ptr, cnt.ptr, None))
     check(vb.lib().vb_synchronize())
+    if want_flags:
+        flags = C.c_uint(0xFFFFFFFF)
+        check(vb.lib().vb_workspace_error_flags(ws.ptr, C.byref(flags), None))
+        return get(V, np.float64), get(cnt, np.uint64), flags.value
     return get(V, np.float64), get(cnt, np.uint64)
 
 

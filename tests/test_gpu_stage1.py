@@ -417,3 +417,71 @@ def test_stage1_on_a_shuffled_pixel_order(case, vb, orc, prec):
     sky0, _ = structs(c, tile=False)
     V0, cnt0 = stage1(sky0, bl, precision=pm, cull=vb.CULL_NONE)
     assert np.array_equal(cnt, cnt0)
+
+
+
+@pytest.mark.parametrize("prec", ["fp32_fp64phase", "fp64", "fp32_dsphase"])
+@pytest.mark.parametrize("cull", ["none", "tilecone", "exact"])
+def test_staging_across_tiles_and_culled_tiles(case, vb, prec, cull):
+    """The pixel records reach shared memory by double-buffered bulk copies
+    (each tile's first stage fetched after the tile's barrier, the next one
+    while the current one is computed; tiles culled for the whole CTA fetch
+    nothing).  Chunks of one tile, of eight tiles and of the automatic size
+    give the same V up to the grouping of the FP64 chunk sums, the same term
+    counters and a clear device error word, with one, two and eight stages
+    per tile."""
+    sky, bl = structs(case)
+    pm = {"fp64": vb.PREC_FP64, "fp32_fp64phase": vb.PREC_FP32_FP64PH, "fp32_dsphase": vb.PREC_FP32_DSPH}[prec]
+    cm = {"none": vb.CULL_NONE, "tilecone": vb.CULL_TILECONE, "exact": vb.CULL_EXACT}[cull]
+    stages = (128, 1024) if cull == "none" else (32, 128, 256)
+    extra = dict(exact_tile_pix=256) if cull == "exact" else {}
+    for st in stages:
+        tile = st if cull == "none" else 256
+        V0, c0, f0 = stage1(sky, bl, precision=pm, cull=cm, stage_pix=st, chunk_pix=tile, want_flags=True, **extra)
+        assert f0 == 0
+        if cull != "none":
+            assert int(c0[2]) > 0, "no culled tile: the skip path would not run"
+        for ch in (8 * tile, 0):
+            V1, c1, f1 = stage1(sky, bl, precision=pm, cull=cm, stage_pix=st, chunk_pix=ch, want_flags=True, **extra)
+            assert f1 == 0, (st, ch, f1)
+            assert np.array_equal(c1, c0), (st, ch)
+            emax, _ = rel_err(V1, V0)
+            assert emax < 2e-6, (st, ch, emax)
+
+
+@pytest.mark.parametrize("drop", [1, 77, 1000])
+def test_stage1_on_a_ragged_pixel_count(case, vb, orc, drop):
+    """A sky whose pixel count is no multiple of the stage (the last stage of
+    the last chunk is short, and so is its bulk copy) gives the FP64 oracle's
+    V, and exact culling on 1024-pixel tiles gives the unculled V bit for bit."""
+    c = case
+    npix = c["npix"] - drop
+    sh = {k: np.ascontiguousarray(c["sky"][k][:npix]) for k in ("B", "l", "m", "n")}
+    dl, dm, dn, dB = (dev(sh[k]) for k in ("l", "m", "n", "B"))
+    sky = sky_struct(dl, dm, dn, dB, npix)
+    bl = bl_struct(c["d"], c["n_full"], c["nbl"], c["cosphi"])
+    Vo = orc.stage1(sh, bl_dict(c), phase_corrected=1, precision=1)
+    for st in (128, 1024):
+        V, cnt, f = stage1(sky, bl, precision=vb.PREC_FP32_FP64PH, cull=vb.CULL_NONE, stage_pix=st, want_flags=True)
+        assert f == 0 and int(cnt[3]) == npix * (c["n_full"] // 2)
+        emax, erms = rel_err(V, Vo)
+        assert emax <= TOL_MIXED and erms <= TOL_MIXED, (st, emax, erms)
+    Ve, ce, fe = stage1(sky, bl, precision=vb.PREC_FP32_FP64PH, cull=vb.CULL_EXACT, exact_tile_pix=1024,
+                        stage_pix=1024, want_flags=True)
+    assert fe == 0 and int(ce[2]) > 0
+    assert np.array_equal(Ve.view(np.uint64), V.view(np.uint64))
+
+
+def test_workspace_alignment_is_checked(case, vb):
+    """A workspace that does not start on a 256-byte boundary is refused on
+    the host before anything is launched (the pixel records are bulk-copied
+    from it, which needs 16-byte aligned addresses)."""
+    from gpu_util import DeviceBuffer
+    sky, bl = structs(case)
+    o = vb.Stage1Opts(precision=vb.PREC_FP32_FP64PH, cull=vb.CULL_TILECONE, phase_corrected=1, blockage=1)
+    need = vb.lib().vb_stage1_workspace_bytes(C.byref(sky), C.byref(bl), C.byref(o))
+    ws = DeviceBuffer(need + 256)
+    V = zeros(case["n_full"], np.float64)
+    rc = vb.lib().vb_viss_halfsym(C.byref(sky), C.byref(bl), C.byref(o), C.c_void_p(ws.ptr + 16), need, V.ptr,
+                                  None, None)
+    assert rc == 1 and b"aligned" in vb.lib().vb_last_error()

@@ -250,16 +250,17 @@ __global__ void k_mask(const float* __restrict__ l, const float* __restrict__ m,
 // Stage-1 pixel records: (l, m) as FP64, (n as FP64 bits, B, nm1), (l, m, n, B).
 __global__ void k_pack_pixels(const float* __restrict__ B, const float* __restrict__ l,
                               const float* __restrict__ m, const float* __restrict__ n,
-                              int64_t npix, double2* __restrict__ lm, float4* __restrict__ nb,
-                              float4* __restrict__ f4) {
+                              int64_t npix, PixRec* __restrict__ px) {
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < npix; i += stride) {
     float lf = l[i], mf = m[i], nf = n[i], bf = B[i];
-    lm[i] = make_double2((double)lf, (double)mf);
+    PixRec r;
+    r.lm = make_double2((double)lf, (double)mf);
     double nd = (double)nf;
-    nb[i] = make_float4(__int_as_float(__double2loint(nd)), __int_as_float(__double2hiint(nd)),
-                        bf, nf - 1.0f);
-    f4[i] = make_float4(lf, mf, nf, bf);
+    r.nb = make_float4(__int_as_float(__double2loint(nd)), __int_as_float(__double2hiint(nd)),
+                       bf, nf - 1.0f);
+    r.f4 = make_float4(lf, mf, nf, bf);
+    px[i] = r;
   }
 }
 
@@ -446,9 +447,9 @@ static int launch_grid(int64_t n, int threads) {
 
 // --- internal entry points used by the pipeline -----------------------------
 int geom_pack_pixels(const float* B, const float* l, const float* m, const float* n,
-                     int64_t npix, double2* lm, float4* nb, float4* f4, cudaStream_t s) {
+                     int64_t npix, PixRec* px, cudaStream_t s) {
   if (npix <= 0) return VB_OK;
-  k_pack_pixels<<<launch_grid(npix, 256), 256, 0, s>>>(B, l, m, n, npix, lm, nb, f4);
+  k_pack_pixels<<<launch_grid(npix, 256), 256, 0, s>>>(B, l, m, n, npix, px);
   VB_LAUNCH_CHECK();
   return VB_OK;
 }

@@ -34,8 +34,16 @@ PhaseMagic phase_magic_for(double max_abs_turns, bool* ok);
 int round_half_away_host(float x);
 void reference_plan(float lambda_m, int* orbit_res, int* nrev, int* seg_len);
 
+// One stage-1 pixel record: FP64 (l, m), (n as two FP64 words, B, n - 1),
+// FP32 (l, m, n, B); 48 bytes, one record per pixel, so that a stage of
+// consecutive pixels is one contiguous range in global and in shared memory.
+struct __align__(16) PixRec {
+  double2 lm;
+  float4 nb;
+  float4 f4;
+};
 int geom_pack_pixels(const float* B, const float* l, const float* m, const float* n, int64_t npix,
-                     double2* lm, float4* nb, float4* f4, cudaStream_t s);
+                     PixRec* px, cudaStream_t s);
 int geom_exact_cones(int tile_pix, const float* l, const float* m, const float* n, int64_t npix,
                      ExactCone* out, cudaStream_t s);
 int geom_validate_async(const float* u, const float* v, const float* w, int n_full, int nbl, int* d_bad,
@@ -55,9 +63,7 @@ struct Stage1Plan {
 };
 
 struct Stage1Buffers {       // slices of a workspace
-  double2* lm = nullptr;
-  float4* nb = nullptr;
-  float4* f4 = nullptr;
+  PixRec* px = nullptr;      // [npix] stage-1 pixel records
   ExactCone* cones = nullptr;
   ExactCone* subcones = nullptr;   // tile-cone refinement sub-tiles
   double2* partial = nullptr;

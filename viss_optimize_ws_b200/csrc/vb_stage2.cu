@@ -1260,6 +1260,8 @@ extern "C" int vb_recon_batched(const vb_sky* sky, const vb_baselines* bl, const
   VB_TRY(stage2_plan(bl->n_full / 2, nseg, sky->npix, o, &p));
   size_t need = stage2_workspace(p, nullptr, 0, nullptr);
   if (!workspace || ws_bytes < need) return fail(VB_ERR_NOMEM, "vb_recon_batched: workspace %zu < %zu", ws_bytes, need);
+  if (reinterpret_cast<uintptr_t>(workspace) % 256 != 0)
+    return fail(VB_ERR_INVALID, "vb_recon_batched: workspace %p is not 256-byte aligned", workspace);
   return stage2_run(sky, bl, V_half, nseg, seg_t0, seg_tlen, p, workspace, ws_bytes, C, W, seg_params, term_counters,
                     nullptr, as_stream(stream), nullptr);
 }
