@@ -208,8 +208,9 @@ typedef struct {
   int ctas_per_sm;      /* resident CTAs per SM the kernel is built for: 2, or 3 with bpt <= 2 (0 = 2) */
   int items_per_cta;    /* work-queue items per resident CTA when chunk_pix = 0 (0 = auto) */
   int refine_pix;       /* tile-cone culling: inside mixed tiles, exact sub-tiles of this many
-                           pixels skip or drop the per-pixel test where they can (0 = 128,
-                           < 0 = off); results are identical either way */
+                           pixels skip or drop the per-pixel test where they can (0 = 256 on
+                           cull tiles of 4096 pixels or more, else 128; < 0 = off); results are
+                           identical either way */
   int mask_visible_tiles; /* tile-cone culling: 0 = tiles the cone test proves visible skip the
                            per-pixel test (upstream's all-visible nm1 fast path,
                            ..._vissfast.cuh:530-539); 1 = they take it like mixed tiles, so
@@ -538,8 +539,8 @@ int vb_make_synthetic_sky(int nside, uint64_t seed, int n_points, float amp, flo
 
 /* Stage-1 tile class of every (half-baseline, cull tile) pair as used by
  * vb_viss_halfsym for opts->cull: 0 hidden, 1 visible (no per-pixel mask),
- * 2 mixed (per-pixel mask).  cls has n_half * ntile bytes, row-major per
- * half-baseline; *ntile_out = number of cull tiles.  Exported for parity
+ * 2 mixed (per-pixel mask).  cls (device memory; VB_ERR_INVALID otherwise) has
+ * n_half * ntile bytes, row-major per half-baseline; *ntile_out = number of cull tiles.  Exported for parity
  * tests (the upstream decision is the inline block at
  * viss_recon_kernel_mirror_tile_vissfast.cuh:519-529). */
 int vb_stage1_tile_classes(const vb_sky* sky, const vb_baselines* bl, const vb_stage1_opts* o,

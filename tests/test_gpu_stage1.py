@@ -485,3 +485,19 @@ def test_workspace_alignment_is_checked(case, vb):
     rc = vb.lib().vb_viss_halfsym(C.byref(sky), C.byref(bl), C.byref(o), C.c_void_p(ws.ptr + 16), need, V.ptr,
                                   None, None)
     assert rc == 1 and b"aligned" in vb.lib().vb_last_error()
+
+
+def test_tile_classes_refuse_a_host_buffer(case, vb):
+    """vb_stage1_tile_classes writes its output with a kernel: a host buffer
+    is refused on the host, before anything is launched."""
+    from gpu_util import DeviceBuffer
+    sky, bl = structs(case)
+    o = vb.Stage1Opts(precision=vb.PREC_FP32_FP64PH, cull=vb.CULL_TILECONE, phase_corrected=1, blockage=1)
+    need = vb.lib().vb_stage1_workspace_bytes(C.byref(sky), C.byref(bl), C.byref(o))
+    ws = DeviceBuffer(need)
+    host = np.zeros((case["n_full"] // 2) * (case["npix"] // 256), dtype=np.uint8)
+    nt = C.c_int()
+    rc = vb.lib().vb_stage1_tile_classes(C.byref(sky), C.byref(bl), C.byref(o), ws.ptr, need, host.ctypes.data,
+                                         C.byref(nt), None)
+    assert rc == 1 and b"device memory" in vb.lib().vb_last_error()
+    assert not host.any()

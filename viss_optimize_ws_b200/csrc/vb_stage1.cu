@@ -90,12 +90,15 @@ __device__ __forceinline__ float rint_magic(float x) {
 
 // VB_CULL_EXACT class of one baseline for one tile.  Kept out of line: the
 // FP64 cone test runs once per (baseline, tile), and inlining it into the
-// persistent kernel costs the pixel loop registers in every cull mode.
+// persistent kernel costs the pixel loop registers in every cull mode.  It
+// uses the FP64 form of the test: with the square-root-free form the kernel
+// ran 8 % slower (out of line) or 15 % slower (inlined) with the same
+// decisions.
 __device__ __noinline__ int exact_tile_class(const ExactCone* cone, float x1, float y1, float z1, float i1, float c1,
                                              float x2, float y2, float z2, float i2, float c2) {
   const ExactCone c = *cone;
-  const int e1 = exact_class(c, x1, y1, z1, i1, c1);
-  const int e2 = exact_class(c, x2, y2, z2, i2, c2);
+  const int e1 = exact_class_fp64(c, x1, y1, z1, i1, c1);
+  const int e2 = exact_class_fp64(c, x2, y2, z2, i2, c2);
   return (e1 < 0 || e2 < 0) ? kClsHid : ((e1 > 0 && e2 > 0) ? kClsVis : kClsMix);
 }
 
@@ -655,13 +658,16 @@ int stage1_plan(const vb_sky* sky, const vb_baselines* bl, const vb_stage1_opts*
   }
   q.stage_pix = stage;
   q.ntile_cull = (int)ceil_div(q.npix, q.cull_tile);
-  // tile-cone culling: exact sub-tiles inside mixed tiles (0 = 128, < 0 = off;
-  // on the nside-256 workload 128-pixel sub-tiles cut the masked terms from
-  // 2.77e9 to 1.44e9 and the kernel time by 6 %)
+  // tile-cone culling: exact sub-tiles inside mixed tiles (0 = automatic,
+  // < 0 = off; on the nside-256 workload 128-pixel sub-tiles cut the masked
+  // terms from 2.77e9 to 1.44e9 and the kernel time by 6 %).  Automatic: 256
+  // pixels on cull tiles of 4096 and more, else 128 (measured on one B200,
+  // 256 against 128: 1220.6 / 1231.9 ms on 16384-pixel tiles, 355.7 / 357.0 ms
+  // on 4096, 9.76 / 9.72 ms and 23.62 / 23.55 ms on 1024)
   q.refine_pix = 0;
   q.mask_visible = (q.cull == VB_CULL_TILECONE && o->mask_visible_tiles) ? 1 : 0;
   if (q.cull == VB_CULL_TILECONE && o->refine_pix >= 0) {
-    int r = o->refine_pix > 0 ? o->refine_pix : 128;
+    int r = o->refine_pix > 0 ? o->refine_pix : (q.cull_tile >= 4096 ? 256 : 128);
     if (!is_pow2(r) || r < 32) return fail(VB_ERR_INVALID, "stage 1: refine_pix=%d (power of two >= 32)", r);
     if (r < q.cull_tile && r <= q.stage_pix) q.refine_pix = r;
   }
@@ -828,6 +834,15 @@ extern "C" int vb_stage1_tile_classes(const vb_sky* sky, const vb_baselines* bl,
   if (ntile_out) *ntile_out = p.ntile_cull;
   if (p.n_half == 0) return VB_OK;
   if (!cls) return fail(VB_ERR_INVALID, "vb_stage1_tile_classes: cls is NULL");
+  {
+    // the classes are written by a kernel: refuse a host buffer up front
+    cudaPointerAttributes at{};
+    if (cudaPointerGetAttributes(&at, cls) != cudaSuccess ||
+        (at.type != cudaMemoryTypeDevice && at.type != cudaMemoryTypeManaged)) {
+      cudaGetLastError();
+      return fail(VB_ERR_INVALID, "vb_stage1_tile_classes: cls %p is not device memory", (void*)cls);
+    }
+  }
   Stage1Buffers b;
   size_t need = stage1_carve(p, nullptr, 0, nullptr, true);
   if (!workspace || ws_bytes < need)

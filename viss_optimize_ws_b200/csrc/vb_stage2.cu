@@ -526,7 +526,9 @@ __device__ __forceinline__ void put_zero(L* list, int k) {
 
 // Exact-cone class of a representative against a pixel block (0 hidden,
 // 1 visible, 2 mixed).  Out of line: it runs once per (group, block) and would
-// otherwise take registers from the term loop.
+// otherwise take registers from the term loop.  The square-root-free test
+// (exact_class) is 1.2 % faster here than the FP64 form on the nside-1024 day
+// (390.9 against 395.8 ms) with the same decisions.
 __device__ __noinline__ int exact_group_class(const ExactCone* cone, float4 p1, float cp1, float4 p2, float cp2) {
   const ExactCone c = *cone;
   const int e1 = exact_class(c, p1.x, p1.y, p1.z, p1.w, cp1);
