@@ -118,6 +118,9 @@ def parse() -> argparse.Namespace:
                          "(strong scaling: stage 1 by time steps + all-gather of V, stage 2 by pixels + gather of C)")
     ap.add_argument("--config", type=int, default=0,
                     help="print a report line for configuration 1-5 instead of the headline line")
+    ap.add_argument("--workload-config", type=int, default=0,
+                    help="time the headline line on configuration N's workload instead (a smaller case of the same "
+                         "kernels for profiler captures; the line then names that workload)")
     ap.add_argument("--day-fraction", type=int, default=1,
                     help="run 1/F of the headline day (time steps and segments divided by F): a smaller case of "
                          "the same kernels for profiler captures; the line then names the reduced workload")
@@ -728,10 +731,16 @@ def main() -> None:
 
     kw = rank_workload_kwargs(local)
     workload = WORKLOAD
+    if args.workload_config:
+        n = args.workload_config
+        kw = dict(config_kwargs(n), device=local)
+        workload = dict(workload=f"config{n}", label=CONFIG_LABELS[n], nside=kw["nside"], npix=12 * kw["nside"] ** 2)
     if args.day_fraction > 1:
+        if "tsteps" not in kw:
+            raise SystemExit("--day-fraction needs a workload with even segments")
         f = args.day_fraction
         kw = dict(kw, tsteps=max(1, kw["tsteps"] // f), segs=max(1, kw["segs"] // f))
-        workload = dict(WORKLOAD, workload=f"{WORKLOAD['workload']}_day1of{f}", tsteps=kw["tsteps"], segs=kw["segs"])
+        workload = dict(workload, workload=f"{workload['workload']}_day1of{f}", tsteps=kw["tsteps"], segs=kw["segs"])
     B = vb.synthetic_sky(kw["nside"], seed=1)
     p, shape_info = tuned_pipeline(vb, kw, B, 16, args.shape)
     shape = shape_string(p.cfg)
@@ -851,8 +860,8 @@ def main() -> None:
                            "peak_source": "MEASURED_PEAKS.json (measured)"}
 
     cpu = None
-    if rank == 0 and ws == 1 and not args.no_cpu:
-        inp = cpu_inputs()
+    if rank == 0 and ws == 1 and not args.no_cpu and args.workload_config in (0, 1, 2, 3, 5):
+        inp = cpu_inputs(args.workload_config or HEADLINE)
         s1, s2 = cpu_sample_sizes(inp, 15.0)
         cs = cpu_sample(inp, s1, s2)
         cpu = dict({"value": cs["value"], "unit": UNIT, "cores": cs["cores"], "kind": "port",

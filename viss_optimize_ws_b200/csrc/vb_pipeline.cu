@@ -951,7 +951,7 @@ extern "C" int vb_pipeline_autotune(vb_pipeline* p, int reps, vb_tune_report* ou
       if (stage > tile) continue;
       for (int ctas : {2, 3}) {
         if (ctas == 3 && bpt > 2) continue;
-        for (int items : {12, 24, 48}) {
+        for (int items : {24, 48, 96}) {
           c.stage1_bpt = bpt; c.stage1_stage_pix = stage; c.stage1_ctas_per_sm = ctas; c.stage1_items_per_cta = items;
           if (plan_stages(p) != VB_OK || time_stages(p, reps, &k1, &k2) != VB_OK) continue;
           ++t.candidates;
