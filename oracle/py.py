@@ -153,10 +153,11 @@ def ptr(a: np.ndarray | None):
 
 
 # --- thin numpy wrappers of the oracle -----------------------------------------
-def nest_lmn_f64(nside: int):
-    n = 12 * nside * nside
+def nest_lmn_f64(nside: int, first: int = 0, count: int | None = None):
+    """FP64 (l, m, n) of NEST pixels [first, first + count) (default: the whole sky)."""
+    n = 12 * nside * nside - first if count is None else count
     l, m, nn = (np.empty(n) for _ in range(3))
-    oracle().or_nest_lmn_f64(nside, 0, n, ptr(l), ptr(m), ptr(nn))
+    oracle().or_nest_lmn_f64(nside, first, n, ptr(l), ptr(m), ptr(nn))
     return l, m, nn
 
 

@@ -153,3 +153,49 @@ def test_orbit_window_and_plan_vs_cpu(gpu, vb, orc):
         vb.lib().vb_orbit_destroy(h)
         assert (orr.value, pc.value, sl.value) == orc.reference_plan(lam)
         assert T.value == pc.value * sl.value and nbl.value == 28
+
+
+@pytest.mark.parametrize("first", [2 ** 31 - 32768, 12 * 16384 ** 2 - 65536])
+def test_nside16384_pixel_indices_beyond_int32(gpu, ref, vb, orc, first):
+    """The upstream's 30 MHz default sky is nside 16384: 3.2e9 pixels, so pixel
+    indices pass 2^31 (main_recon_online.cu:33-37).  For 65,536 pixels that
+    straddle 2^31 (the end of face 7 and the south-polar start of face 8) and
+    for the last 65,536 of the sky, the geometry is bit-identical to the
+    upstream kernel's, and stage 1 over those pixels matches the FP64 oracle
+    (with exact culling bit-identical to none).
+
+    Against the FP64 restatement the float geometry is within 4e-6, except
+    close to a pole: the upstream formula takes sin(theta) from a float z, so
+    l and m carry an error of about ulp(z) / sin(theta) there (2e-4 at the
+    pixels next to the pole at this nside), which the bound follows."""
+    from conftest import rel_err
+    from gpu_util import bl_struct, reference_baselines, sky_struct, stage1
+    nside, cnt = 16384, 65536
+    cl, cm, cn = zeros(cnt), zeros(cnt), zeros(cnt)
+    vb.check(vb.lib().vb_pix2lmn_nest(nside, first, cnt, cl.ptr, cm.ptr, cn.ptr, None))
+    rl, rm, rn = zeros(cnt), zeros(cnt), zeros(cnt)
+    assert ref.ref_root().ref_pix2lmn(nside, first, cnt, vp(rl), vp(rm), vp(rn)) == 0
+    l, m, n = get(cl), get(cm), get(cn)
+    for a, b in ((l, get(rl)), (m, get(rm)), (n, get(rn))):
+        assert np.array_equal(bits(a), bits(b))
+    L, M, N = orc.nest_lmn_f64(nside, first, cnt)
+    bound = 4e-6 + 4e-7 / np.maximum(np.hypot(L, M), 1e-12)
+    assert (np.abs(l - L) <= bound).all() and (np.abs(m - M) <= bound).all()
+    assert np.abs(n - N).max() < 4e-6
+    B = (np.random.default_rng(11).random(cnt) * 1e-3).astype(np.float32)
+    dB = dev(B)                                   # held for as long as the sky refers to it
+    sky = sky_struct(cl, cm, cn, dB, cnt)
+    host, d = reference_baselines(float(np.float32(300.0)), 1, 42, 2000, 16)
+    n_full = host["u"].size
+    bl = bl_struct(d, n_full, 28, upstream_cosphi())
+    V, c, f = stage1(sky, bl, precision=vb.PREC_FP32_FP64PH, cull=vb.CULL_NONE, want_flags=True)
+    assert f == 0 and int(c[3]) == cnt * (n_full // 2)
+    Vo = orc.stage1(dict(B=B, l=l, m=m, n=n), dict(host, cosphi=upstream_cosphi()), phase_corrected=1, precision=1)
+    if np.abs(Vo).max() > 0:
+        emax, erms = rel_err(V, Vo)
+        assert emax <= 1e-5 and erms <= 1e-5, (emax, erms)
+    else:                                         # every pixel hidden from every baseline
+        assert np.abs(V).max() == 0
+    Ve, ce, fe = stage1(sky, bl, precision=vb.PREC_FP32_FP64PH, cull=vb.CULL_EXACT, exact_tile_pix=1024,
+                        stage_pix=1024, want_flags=True)
+    assert fe == 0 and np.array_equal(Ve.view(np.uint64), V.view(np.uint64))

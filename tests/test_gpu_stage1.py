@@ -433,7 +433,8 @@ def test_staging_across_tiles_and_culled_tiles(case, vb, prec, cull):
     sky, bl = structs(case)
     pm = {"fp64": vb.PREC_FP64, "fp32_fp64phase": vb.PREC_FP32_FP64PH, "fp32_dsphase": vb.PREC_FP32_DSPH}[prec]
     cm = {"none": vb.CULL_NONE, "tilecone": vb.CULL_TILECONE, "exact": vb.CULL_EXACT}[cull]
-    stages = (128, 1024) if cull == "none" else (32, 128, 256)
+    # 2048: the largest stage, two 96 KB buffers, one CTA per SM
+    stages = (128, 1024, 2048) if cull == "none" else (32, 128, 256)
     extra = dict(exact_tile_pix=256) if cull == "exact" else {}
     for st in stages:
         tile = st if cull == "none" else 256
