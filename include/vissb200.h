@@ -358,7 +358,7 @@ typedef struct vb_pipeline vb_pipeline;
 
 typedef struct {
   /* upstream flags (main_recon_online.cu:6-27, ..._mirror_tile_vissfast.cu:7-31) */
-  int      nside;
+  int      nside;          /* power of two <= 16384 (3.2e9 pixels: beyond one device, use slab_pix) */
   int      day;
   int      segs;
   int      blockage;

@@ -176,3 +176,38 @@ def test_dropin_sky_slab_streaming(gpu, vb, tmp_path):
     acc = np.fromfile(b / "sum.bin", dtype=np.float32)
     ref = sum(np.fromfile(b / f"C{d}day1M.bin", dtype=np.float32).astype(np.float64) for d in (1, 2))
     assert np.abs(acc - ref).max() <= 1e-6 * np.abs(ref).max()
+
+
+def test_dropin_30mhz_default_sky_streams_in_slabs(gpu, vb, tmp_path):
+    """The upstream's 30 MHz runs use nside 16384 (3.2e9 pixels; its 30 MHz
+    scripts pass --nside=16384, and --nside=0 picks it from --btag=30M,
+    main_recon_online.cu:33-37), whose stage-1 records alone need ~150 GB: the
+    drop-in finds that the resident sky does not fit and streams it in slabs
+    by itself.  A short synthetic day (4 satellites x 16 steps) keeps it quick;
+    C at 4096 sampled pixels equals the Python API's run with the same slabs."""
+    import re
+    exe = BIN / "main_recon_online_mirror_tile_vissfast"
+    out = tmp_path / "out"
+    args = ["--btag=30M", "--nside=16384", "--segs=2", "--blockage=1", "--occ_mode=2", f"--sky_dir={tmp_path}/sky", "--gpus=0",
+            "--B_mode=bin", "--C_mode=bin", "--orbit_seed=42", "--sky_gen=5", "--orbit_model=synthetic", "--nsat=4",
+            "--tsteps=16", "--occ_R_m=6371e3", "--grid_res=65", "--bl_max_m=0", f"--out_dir={out}/"]
+    r = run(exe, args, tmp_path)
+    assert r.returncode == 0, r.stderr[-2000:]
+    m = re.search(r"streaming it in slabs of (\d+) pixels", r.stdout)
+    assert m, r.stdout[-2000:]
+    slab = int(m.group(1))
+    npix = 12 * 16384 ** 2
+    Cfile = out / "C1day30M.bin"
+    assert Cfile.stat().st_size == 4 * npix
+    idx = np.sort(np.random.default_rng(2).choice(npix, 4096, replace=False))
+    Cd = np.memmap(Cfile, dtype=np.float32, mode="r")[idx].copy()
+    assert np.isfinite(Cd).all() and np.abs(Cd).max() > 0
+    B = vb.synthetic_sky(16384, seed=5)
+    kw = dict(nside=16384, orbit_model=vb.ORBIT_SYNTHETIC, nsat=4, tsteps=16, segs=2, lambda_m=vb.btag_lambda("30M"),
+              occ_R_m=6371e3, cull="tilecone", viss_tile_pix=256, mirror=1, grid_res=65, bl_max_m=0.0,
+              occ_mode=2, blockage=1, orbit_seed=42, slab_pix=slab)
+    with vb.Pipeline(vb.run_config(**kw)) as p:
+        Cp, _, rep = p.run_host(B)
+    assert rep["error_flags"] == 0
+    e = rel_err(Cd, Cp[idx])
+    assert e[0] < 1e-6 and e[1] < 1e-6, e

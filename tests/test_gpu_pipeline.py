@@ -324,3 +324,54 @@ def test_sky_slab_size_must_hold_whole_tiles(gpu, vb):
         vb.Pipeline(vb.run_config(nside=32, orbit_model=vb.ORBIT_SYNTHETIC, nsat=4, tsteps=8, segs=2,
                                   lambda_m=30.0, occ_R_m=6371e3, cull="tilecone", viss_tile_pix=2048,
                                   slab_pix=3072))
+
+
+def test_nside16384_day_in_sky_slabs(gpu, vb, orc):
+    """The upstream's 30 MHz default sky is nside 16384 (3.2e9 pixels,
+    main_recon_online.cu:33-37), larger than the device holds with its stage-1
+    records.  The pipeline streams it in 12 slabs of 2^28 pixels; the sky is
+    one point source at pixel 2,750,722,240 (past 2^31) and 4 satellites give
+    96 half-baselines.  V is that one pixel's terms: within 1e-5 of the FP64
+    oracle on the one-pixel sky, so |V_k| is B where both endpoints see the
+    source and 0 where either does not.  C at the source and its neighbours
+    matches the oracle's stage 2 on those pixels with the pipeline's V and
+    segments, and the term counters hold npix x N_half (past 2^32).  Visible
+    tiles take the per-pixel test here (nm1_fast=0), so the one-pixel oracle
+    sees the same masks."""
+    from gpu_util import get, zeros
+    nside = 16384
+    npix = 12 * nside * nside
+    src = 2_750_722_240                      # seen by about half of the baselines
+    kw = dict(nside=nside, orbit_model=vb.ORBIT_SYNTHETIC, nsat=4, tsteps=16, segs=2,
+              lambda_m=vb.btag_lambda("30M"), occ_R_m=6371e3, cull="tilecone", viss_tile_pix=16384, mirror=1,
+              grid_res=65, bl_max_m=0.0, nm1_fast=0, slab_pix=1 << 28)
+    B = np.zeros(npix, dtype=np.float32)
+    B[src] = 1.0
+    with vb.Pipeline(vb.run_config(**kw)) as p:
+        assert p.npix == npix
+        Cout, V, rep = p.run_host(B, scale=False, want_v=True)
+        keys = ("u", "v", "w", "x1", "y1", "z1", "x2", "y2", "z2", "invn1", "invn2", "cosphi1", "cosphi2")
+        bl = {k: p.get(k) for k in keys}
+        bl["nbl"], bl["cosphi"] = p.nbl, p.cosphi
+        t0, tl = p.seg_plan()
+        n_half = p.n_half
+    del B
+    assert rep["error_flags"] == 0
+    assert rep["s1_counters"][3] == npix * n_half and rep["stage1_terms"] == npix * n_half
+    # geometry of the source and its neighbours (bit-identical to the upstream kernel's)
+    g = [zeros(9) for _ in range(3)]
+    vb.check(vb.lib().vb_pix2lmn_nest(nside, src - 4, 9, g[0].ptr, g[1].ptr, g[2].ptr, None))
+    l, m, n = (get(a) for a in g)
+    one = dict(B=np.ones(1, np.float32), l=l[4:5], m=m[4:5], n=n[4:5])
+    Vo = orc.stage1(one, bl, phase_corrected=1, precision=1)
+    emax, erms = rel_err(V, Vo)
+    assert emax <= TOL and erms <= TOL, (emax, erms)
+    mag = np.hypot(V[0::2], V[1::2])
+    seen = mag > 0.5
+    assert seen.any() and (~seen).any()                    # both visible and occluded baselines
+    assert np.abs(mag[seen] - 1.0).max() < 1e-5 and mag[~seen].max() == 0.0
+    sky9 = dict(l=l, m=m, n=n)
+    Co, Wo, _ = orc.stage2(sky9, bl, V, t0, tl, mirror=1, blockage=1, occ_mode=2, bl_max=rep["bl_max_m"],
+                           lam=kw["lambda_m"], grid_res=kw["grid_res"], precision=1)
+    emax, erms = rel_err(Cout[src - 4:src + 5], Co)
+    assert emax <= TOL and erms <= TOL, (emax, erms)

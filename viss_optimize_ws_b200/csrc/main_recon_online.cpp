@@ -320,7 +320,33 @@ int main(int argc, char** argv) {
     Timer t_init;
     t_init.tic();
     if (!p) {
-      if (vb_pipeline_create(&cfg, &p) != VB_OK) return die(std::string("ERROR ") + vb_last_error());
+      int rc = vb_pipeline_create(&cfg, &p);
+      if (rc == VB_ERR_NOMEM && !slab_pix) {
+        // The sky does not fit on the device with its stage-1 records (the
+        // upstream's 30 MHz sky, nside 16384, needs ~320 GB resident): stream
+        // it through in slabs of whole cull tiles and stage-2 pixel blocks, a
+        // power of two half the largest that fits, so that the running sum
+        // and the rest of the run keep room on the device.
+        const long long unit = std::max<long long>(1024, cfg.viss_tile_pix > 0 ? cfg.viss_tile_pix : 256);
+        long long s = 1;
+        while (s * 2 <= npix / 2) s *= 2;
+        for (; s >= unit && rc == VB_ERR_NOMEM; s /= 2) {
+          cfg.slab_pix = s;
+          rc = vb_pipeline_create(&cfg, &p);
+          if (rc == VB_OK) slab_pix = s;
+        }
+        if (rc == VB_OK && slab_pix / 2 >= unit) {
+          vb_pipeline_destroy(p);
+          p = nullptr;
+          cfg.slab_pix = slab_pix / 2;
+          rc = vb_pipeline_create(&cfg, &p);
+          if (rc == VB_OK) slab_pix = cfg.slab_pix;
+        }
+        if (rc == VB_OK)
+          std::cout << "Sky of " << npix << " pixels does not fit on the device: streaming it in slabs of "
+                    << slab_pix << " pixels\n";
+      }
+      if (rc != VB_OK) return die(std::string("ERROR ") + vb_last_error());
       if (!slab_pix && vb_pipeline_set_sky(p, hB.data(), 1) != VB_OK)
         return die(std::string("ERROR ") + vb_last_error());
       if (!accum_file.empty()) {

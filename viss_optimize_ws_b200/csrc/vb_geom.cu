@@ -612,6 +612,7 @@ extern "C" int vb_orbit_create(const vb_orbit_params* p, vb_orbit** out) {
   size_t tab = (size_t)o->nrows * o->nsat * sizeof(float);
   auto chk = [&](cudaError_t e, const char* what) {
     if (e != cudaSuccess && rc == VB_OK) rc = cuda_fail(e, what, __FILE__, __LINE__);
+    if (e != cudaSuccess) cudaGetLastError();   // reported once, here
   };
   chk(cudaMalloc(&o->X, tab), "cudaMalloc X");
   chk(cudaMalloc(&o->Y, tab), "cudaMalloc Y");

@@ -175,8 +175,13 @@ static int dalloc(vb_pipeline* p, T** ptr, size_t count) {
   *ptr = nullptr;
   if (count == 0) count = 1;
   cudaError_t e = cudaMalloc(reinterpret_cast<void**>(ptr), count * sizeof(T));
-  if (e != cudaSuccess)
+  if (e != cudaSuccess) {
+    // a failed allocation also sets the runtime's last-error state: clear it, so
+    // that the next launch check does not report it as a kernel failure (a
+    // caller may retry smaller, e.g. with sky slabs)
+    cudaGetLastError();
     return fail(VB_ERR_NOMEM, "cudaMalloc of %zu bytes failed: %s", count * sizeof(T), cudaGetErrorString(e));
+  }
   p->owned.push_back(*ptr);
   return VB_OK;
 }
@@ -330,8 +335,10 @@ static vb_orbit_params orbit_params_of(const vb_run_config& c) {
 extern "C" int vb_pipeline_create(const vb_run_config* c, vb_pipeline** out) {
   if (!c || !out) return fail(VB_ERR_INVALID, "vb_pipeline_create: null argument");
   *out = nullptr;
-  if (c->nside <= 0 || (c->nside & (c->nside - 1)) || c->nside > 8192)
-    return fail(VB_ERR_INVALID, "nside=%d must be a power of two <= 8192", c->nside);
+  // up to the upstream's 30 MHz sky (nside 16384, 3.2e9 pixels: past 2^31, so every
+  // pixel offset here is 64-bit; at that size the sky streams through in slabs)
+  if (c->nside <= 0 || (c->nside & (c->nside - 1)) || c->nside > 16384)
+    return fail(VB_ERR_INVALID, "nside=%d must be a power of two <= 16384", c->nside);
   if (c->precision < VB_PREC_REF32 || c->precision > VB_PREC_FP32_DSPH)
     return fail(VB_ERR_INVALID, "precision=%d", c->precision);
   VB_CUDA(cudaSetDevice(c->device));
@@ -1191,7 +1198,10 @@ extern "C" int vb_malloc(void** ptr, size_t bytes) {
   if (!ptr) return fail(VB_ERR_INVALID, "vb_malloc: null ptr");
   *ptr = nullptr;
   cudaError_t e = cudaMalloc(ptr, bytes ? bytes : 1);
-  if (e != cudaSuccess) return fail(VB_ERR_NOMEM, "vb_malloc(%zu): %s", bytes, cudaGetErrorString(e));
+  if (e != cudaSuccess) {
+    cudaGetLastError();   // the failed allocation is reported here, not by the next launch check
+    return fail(VB_ERR_NOMEM, "vb_malloc(%zu): %s", bytes, cudaGetErrorString(e));
+  }
   return VB_OK;
 }
 extern "C" int vb_free(void* ptr) {
