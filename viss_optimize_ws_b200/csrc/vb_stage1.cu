@@ -78,6 +78,7 @@ struct Baseline {
   float uf, vf, wf, fw;   // FP32 copies; fw = -frac(w) (raw phase, DS)
   float ku, kv, kw;       // REF32: -2 pi * (u, v, w)
   float x1, y1, z1, i1, x2, y2, z2, i2, c1, c2;
+  float t1, t2;   // occ_threshold of (i1, c1), (i2, c2)
   float ux1, uy1, uz1, ux2, uy2, uz2;
   int cls;    // class the pixel loop uses (tile class, or the sub-tile class when refined)
   int tcls;   // tile class (decides whether the staged partials are kept)
@@ -134,6 +135,27 @@ __device__ __forceinline__ int tile_class_rt(const S1Args& a, const Baseline& b,
 
 // Loads half-baseline ih into registers (upstream: viss_recon_kernel.cuh:231-240,
 // ..._vissfast.cuh:476-497).
+
+// Per-endpoint threshold of the per-pixel occlusion test: the test
+// "fl(d * invn) < cosphi" (d the FP32 dot of pixel and endpoint, rounded as
+// occ_dot rounds it) holds exactly when d < t, t being the smallest float with
+// fl(t * invn) >= cosphi: fl(d * invn) does not decrease as d grows (invn > 0).
+// The masked path then compares d with t instead of multiplying first, with
+// the same masks (two multiplies fewer per masked term: 1217.7 -> 1206.1 ms on
+// the nside-1024 day, 9.66 -> 9.64 ms at nside 256).
+__device__ __noinline__ float occ_threshold(float invn, float c) {
+  if (c != c || invn != invn) return -INFINITY;                  // the test never fails
+  if (invn == 0.0f) return c > 0.0f ? INFINITY : -INFINITY;      // fl(d * 0) = 0 against c
+  if (isinf(invn)) return 0.0f;                                  // d * inf: fails exactly for d < 0
+  float t = c / invn;                                            // within a few ulps; fixed below
+  for (int k = 0; k < 16 && !(t * invn >= c); ++k) t = nextafterf(t, INFINITY);
+  for (int k = 0; k < 16; ++k) {
+    const float p = nextafterf(t, -INFINITY);
+    if (p * invn >= c) t = p; else break;
+  }
+  return t;
+}
+
 __device__ __forceinline__ void load_baseline(const S1Args& a, int ih, bool raw, Baseline& b) {
   b.active = ih < a.n_half;
   const int i = b.active ? half_to_full_pos(ih, a.nbl) : 0;
@@ -153,6 +175,8 @@ __device__ __forceinline__ void load_baseline(const S1Args& a, int ih, bool raw,
     b.x1 = b.y1 = b.z1 = b.i1 = b.x2 = b.y2 = b.z2 = b.i2 = 0.f;
     b.c1 = b.c2 = a.cosphi;
   }
+  b.t1 = occ_threshold(b.i1, b.c1);
+  b.t2 = occ_threshold(b.i2, b.c2);
   b.ux1 = b.x1 * b.i1; b.uy1 = b.y1 * b.i1; b.uz1 = b.z1 * b.i1;
   b.ux2 = b.x2 * b.i2; b.uy2 = b.y2 * b.i2; b.uz2 = b.z2 * b.i2;
   b.cls = b.tcls = kClsHid;
@@ -404,9 +428,9 @@ __global__ void __maxnreg__(MINB == 3 ? 80 : 120) k_stage1(const S1Args a) {
             const Baseline& b = bl[k];
             bool inc = true;
             if constexpr (MASKED) {
-              const float o1 = occ_dot(f.x, f.y, f.z, b.x1, b.y1, b.z1, b.i1);
-              const float o2 = occ_dot(f.x, f.y, f.z, b.x2, b.y2, b.z2, b.i2);
-              const bool pass = !(o1 < b.c1 || o2 < b.c2);
+              const float d1 = f.x * b.x1 + f.y * b.y1 + f.z * b.z1;
+              const float d2 = f.x * b.x2 + f.y * b.y2 + f.z * b.z2;
+              const bool pass = !(d1 < b.t1 || d2 < b.t2);
               inc = (b.cls == kClsVis) || (b.cls == kClsMix && pass);
             } else if constexpr (PATH == 1) {
               inc = (b.cls != kClsHid);
