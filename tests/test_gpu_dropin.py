@@ -185,12 +185,20 @@ def test_dropin_30mhz_default_sky_streams_in_slabs(gpu, vb, tmp_path):
     drop-in finds that the resident sky does not fit and streams it in slabs
     by itself.  A short synthetic day (4 satellites x 16 steps) keeps it quick;
     C at 4096 sampled pixels equals the Python API's run with the same slabs."""
-    import re
     exe = BIN / "main_recon_online_mirror_tile_vissfast"
     out = tmp_path / "out"
     args = ["--btag=30M", "--nside=16384", "--segs=2", "--blockage=1", "--occ_mode=2", f"--sky_dir={tmp_path}/sky", "--gpus=0",
             "--B_mode=bin", "--C_mode=bin", "--orbit_seed=42", "--sky_gen=5", "--orbit_model=synthetic", "--nsat=4",
             "--tsteps=16", "--occ_R_m=6371e3", "--grid_res=65", "--bl_max_m=0", f"--out_dir={out}/"]
+    try:
+        _check_30mhz_run(vb, exe, args, out, tmp_path)
+    finally:                                  # the sky and C files are 12.9 GB each
+        for f in (tmp_path / "sky" / "B_30M.bin", out / "C1day30M.bin"):
+            f.unlink(missing_ok=True)
+
+
+def _check_30mhz_run(vb, exe, args, out, tmp_path):
+    import re
     r = run(exe, args, tmp_path)
     assert r.returncode == 0, r.stderr[-2000:]
     m = re.search(r"streaming it in slabs of (\d+) pixels", r.stdout)
