@@ -210,3 +210,52 @@ def test_sky_generator_matches_library(orc, vb):
     b = vb.synthetic_sky(8, seed=11, n_points=20, amp=10.0)
     assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
     assert a.min() >= 0 and (a >= 10).sum() >= 15
+
+
+def _occ_threshold(invn: np.float32, c: np.float32) -> np.float32:
+    """The stage-1 kernel's per-endpoint threshold (occ_threshold), restated in
+    numpy float32: the smallest float t with fl(t * invn) >= c."""
+    f = np.float32
+    if np.isnan(c) or np.isnan(invn):
+        return f(-np.inf)
+    if invn == 0:
+        return f(np.inf) if c > 0 else f(-np.inf)
+    if np.isinf(invn):
+        return f(0.0)
+    t = f(c / invn)
+    for _ in range(16):
+        if f(t * invn) >= c:
+            break
+        t = np.nextafter(t, f(np.inf))
+    for _ in range(16):
+        p = np.nextafter(t, f(-np.inf))
+        if f(p * invn) >= c:
+            t = p
+        else:
+            break
+    return t
+
+
+def test_occlusion_threshold_is_exact():
+    """The per-pixel occlusion test fl(d * invn) < cosphi is decided in the
+    stage-1 kernel as d < t with a per-endpoint float threshold t.  Rounding to
+    nearest never decreases as d grows (invn > 0), so the two tests agree for
+    every d: checked for random endpoints' invn and horizon cosines, on random
+    d and on the 64 floats either side of each threshold, where a slip in t
+    would show."""
+    rng = np.random.default_rng(17)
+    f = np.float32
+    for _ in range(400):
+        invn = f(1.0 / rng.uniform(1700.0, 45000.0))          # 1 / |endpoint| in km
+        c = f(rng.uniform(-1.0, 1.0))
+        t = _occ_threshold(invn, c)
+        assert f(t * invn) >= c and f(np.nextafter(t, f(-np.inf)) * invn) < c
+        d = rng.uniform(-5e4, 5e4, 2000).astype(np.float32)
+        near = [t]
+        for _ in range(64):
+            near.append(np.nextafter(near[-1], f(np.inf)))
+        lo = [t]
+        for _ in range(64):
+            lo.append(np.nextafter(lo[-1], f(-np.inf)))
+        d = np.concatenate([d, np.array(near + lo, dtype=np.float32)])
+        assert np.array_equal((d * invn).astype(np.float32) < c, d < t)
