@@ -411,6 +411,7 @@ __global__ void __maxnreg__(MINB == 3 ? 80 : 120) k_stage1(const S1Args a) {
         // baseline by its class (visible or hidden, no per-pixel test); 2: the
         // per-pixel occlusion test for mixed baselines (visible ones included
         // unconditionally, hidden excluded)
+        float e1[BPT], e2[BPT];   // thresholds with the class folded in (masked path)
         auto pixel = [&](const int j, float (&aR)[BPT], float (&aI)[BPT], auto path_tag, auto par_tag) {
           constexpr int PATH = decltype(path_tag)::value;
           constexpr bool MASKED = (PATH == 2);
@@ -430,8 +431,7 @@ __global__ void __maxnreg__(MINB == 3 ? 80 : 120) k_stage1(const S1Args a) {
             if constexpr (MASKED) {
               const float d1 = f.x * b.x1 + f.y * b.y1 + f.z * b.z1;
               const float d2 = f.x * b.x2 + f.y * b.y2 + f.z * b.z2;
-              const bool pass = !(d1 < b.t1 || d2 < b.t2);
-              inc = (b.cls == kClsVis) || (b.cls == kClsMix && pass);
+              inc = !(d1 < e1[k] || d2 < e2[k]);
             } else if constexpr (PATH == 1) {
               inc = (b.cls != kClsHid);
             }
@@ -457,6 +457,18 @@ __global__ void __maxnreg__(MINB == 3 ? 80 : 120) k_stage1(const S1Args a) {
 
         // pixels [j0, j1) of the staged tile (j0 even: pixel parity = index parity)
         auto run = [&](const int j0, const int j1, auto path_tag) {
+          if constexpr (decltype(path_tag)::value == 2) {
+            // masked path: fold each baseline's class into its thresholds, so
+            // that inclusion is one pair of comparisons (visible: -inf, always
+            // in; hidden: +inf, never in for a finite dot; a hidden class comes
+            // only from cone tests on finite endpoints, whose dots are finite)
+#pragma unroll
+            for (int k = 0; k < BPT; ++k) {
+              const int c = bl[k].cls;
+              e1[k] = c == kClsMix ? bl[k].t1 : (c == kClsVis ? -INFINITY : INFINITY);
+              e2[k] = c == kClsMix ? bl[k].t2 : (c == kClsVis ? -INFINITY : INFINITY);
+            }
+          }
           int j = j0;
           // two pixel pairs per trip: 0.5 % faster than the compiler's choice
           // (no unroll 1: +5 %, unroll 3 / 4: +5-6 %)
